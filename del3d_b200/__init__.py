@@ -1,0 +1,373 @@
+"""del3d_b200 - del3d's Delaunay::build hot path on B200 (sm_100a).
+
+Python host side over the C ABI of ``libdel3d_b200.so`` (``include/del3d_b200.h``).
+It mirrors the reference's public interface (``include/del3d/delaunay.h``,
+``predicates.h``, ``predicates2.h``, ``spatial_sort.h`` in the del3d tree):
+
+* :class:`Delaunay` - ``build(points)``, ``finite_cells()``, ``all_cells()``,
+  ``incident_cells()``, ``number_of_vertices()``;
+* :func:`orient3d`, :func:`in_sphere`, :func:`in_sphere_unperturbed`,
+  :func:`orient2d`, :func:`coplanar_orientation`, :func:`coplanar_in_circle`,
+  :func:`coplanar_in_circle_unperturbed`, :func:`collinear` - batched over index
+  tuples into one point table;
+* :func:`spatial_sort` - the reference insertion order, bit for bit.
+
+Everything runs on the GPU; there is no CPU fallback.  Importing works without a
+GPU (the library loads), but every call then fails with :class:`Del3dError`.
+
+One documented difference: ``finite_cells()`` comes back in a canonical order
+(each tet rotated by an even permutation so its smallest index leads, tets
+sorted lexicographically) instead of the reference's cell-allocation order; the
+set of tets is the reference's.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+__all__ = [
+    "Del3dError", "Delaunay", "Point3", "orient3d", "in_sphere", "in_sphere_unperturbed",
+    "orient2d", "coplanar_orientation", "coplanar_in_circle", "coplanar_in_circle_unperturbed",
+    "collinear", "spatial_sort", "library", "LIB_PATH", "predicate_stats",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdel3d_b200.so")
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I32 = ctypes.c_int32
+_INT = ctypes.c_int
+
+
+class Del3dError(RuntimeError):
+    """A non-OK status from the C ABI (the reference has no error channel; this
+    library never fails silently)."""
+
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        msg = f"{where}: {_status_string(status)}"
+        if detail:
+            msg += f" ({detail})"
+        super().__init__(msg)
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [
+        ("n_points", _I64), ("n_vertices", _I64), ("n_cells", _I64),
+        ("cells", ctypes.POINTER(_I32)), ("n_all", _I64), ("all_cells", ctypes.POINTER(_I32)),
+        ("incident_offsets", ctypes.POINTER(_I64)), ("incident", ctypes.POINTER(_I32)),
+        ("rounds", _I32), ("n_exact", _I64), ("device_ms", ctypes.c_double),
+    ]
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("want_all_cells", _I32), ("want_incident", _I32), ("chunk", _I32),
+                ("max_rounds", _I32)]
+
+
+class _PredStats(ctypes.Structure):
+    _fields_ = [("n_queries", _I64), ("n_exact", _I64)]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def library() -> ctypes.CDLL:
+    """The loaded C library.  Raises if it was not built (``python -c
+    'import __graft_entry__ as g; g.build()'``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"del3d_b200: {LIB_PATH} is missing; build it with __graft_entry__.build()")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.d3g_status_string.argtypes = [_INT]
+    lib.d3g_status_string.restype = ctypes.c_char_p
+    lib.d3g_last_error.argtypes = []
+    lib.d3g_last_error.restype = ctypes.c_char_p
+    lib.d3g_predicate_arity.argtypes = [_INT]
+    lib.d3g_predicate_arity.restype = _INT
+    lib.d3g_predicates.argtypes = [_P, _I64, _P, _I64, _INT, _P, ctypes.POINTER(_PredStats)]
+    lib.d3g_predicates_device.argtypes = [_P, _I64, _P, _I64, _INT, _P, _P, ctypes.POINTER(_PredStats)]
+    lib.d3g_orient2d.argtypes = [_P, _I64, _P]
+    lib.d3g_spatial_sort.argtypes = [_P, _I64, _P]
+    lib.d3g_spatial_sort_device.argtypes = [_P, _I64, _P, _P]
+    lib.d3g_shuffle_device.argtypes = [_I64, _P, _P]
+    lib.d3g_options_default.argtypes = [ctypes.POINTER(_Options)]
+    lib.d3g_build.argtypes = [_P, _I64, ctypes.POINTER(_Options), ctypes.POINTER(_Result)]
+    lib.d3g_result_free.argtypes = [ctypes.POINTER(_Result)]
+    lib.d3g_build_device.argtypes = [_P, _I64, ctypes.POINTER(_Options), _P, _I64,
+                                     ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P]
+    lib.d3g_gen_uniform.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, _P]
+    lib.d3g_gen_sphere.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, _I32, _P]
+    lib.d3g_gen_clusters.argtypes = [_I64, ctypes.c_uint32, _I32, ctypes.c_double, _P]
+    lib.d3g_gen_lattice.argtypes = [_I64, _P]
+    for name in ("d3g_predicates", "d3g_predicates_device", "d3g_orient2d", "d3g_spatial_sort",
+                 "d3g_spatial_sort_device", "d3g_shuffle_device", "d3g_build", "d3g_build_device"):
+        getattr(lib, name).restype = _INT
+    _lib = lib
+    return lib
+
+
+def _status_string(status: int) -> str:
+    try:
+        return library().d3g_status_string(status).decode()
+    except ImportError:
+        return f"status {status}"
+
+
+def _check(status: int, where: str) -> None:
+    if status != 0:
+        detail = library().d3g_last_error().decode()
+        raise Del3dError(status, where, detail)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _points(points) -> np.ndarray:
+    """(n, 3) float64 C-contiguous view/copy of `points` (array-like or Point3 list)."""
+    if isinstance(points, np.ndarray):
+        a = points
+    elif len(points) and hasattr(points[0], "x"):
+        a = np.array([(p.x, p.y, p.z) for p in points], dtype=np.float64)
+    else:
+        a = np.asarray(points, dtype=np.float64)
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 3)
+    return a
+
+
+class Point3:
+    """A point (reference ``include/del3d/spatial_sort.h:31``)."""
+
+    __slots__ = ("x", "y", "z")
+
+    def __init__(self, x: float, y: float, z: float):
+        self.x, self.y, self.z = float(x), float(y), float(z)
+
+    def __iter__(self):
+        yield self.x
+        yield self.y
+        yield self.z
+
+    def __repr__(self) -> str:
+        return f"Point3({self.x!r}, {self.y!r}, {self.z!r})"
+
+
+# ---- predicates -----------------------------------------------------------------
+
+ORIENT3D, IN_SPHERE, IN_SPHERE_UNPERTURBED = 0, 1, 2
+COPLANAR_ORIENTATION3, COPLANAR_ORIENTATION4 = 3, 4
+COPLANAR_IN_CIRCLE, COPLANAR_IN_CIRCLE_UNPERTURBED, COLLINEAR = 5, 6, 7
+
+_last_pred_stats = (0, 0)
+
+
+def predicate_stats():
+    """(queries, queries that reached the exact stage) of the last predicate call."""
+    return _last_pred_stats
+
+
+def _predicate(kind: int, points, idx) -> np.ndarray:
+    global _last_pred_stats
+    lib = library()
+    pts = _points(points)
+    k = lib.d3g_predicate_arity(kind)
+    ix = np.ascontiguousarray(idx, dtype=np.int32).reshape(-1, k)
+    if kind == ORIENT3D and ix.ctypes.data % 16:
+        ix = np.array(ix, dtype=np.int32, copy=True, order="C")
+    out = np.zeros(ix.shape[0], dtype=np.int8)
+    st = _PredStats()
+    _check(lib.d3g_predicates(_ptr(pts), pts.shape[0], _ptr(ix), ix.shape[0], kind, _ptr(out),
+                              ctypes.byref(st)), "predicates")
+    _last_pred_stats = (st.n_queries, st.n_exact)
+    return out
+
+
+def orient3d(points, idx) -> np.ndarray:
+    """Sign of |b-a, c-a, d-a| per row (a, b, c, d) of `idx` (reference predicates.h:28)."""
+    return _predicate(ORIENT3D, points, idx)
+
+
+def in_sphere(points, idx) -> np.ndarray:
+    """Perturbed in-sphere per row (a, b, c, d, e); never 0 (reference predicates.h:52)."""
+    return _predicate(IN_SPHERE, points, idx)
+
+
+def in_sphere_unperturbed(points, idx) -> np.ndarray:
+    """Raw in-sphere per row; 0 when cospherical (reference predicates.h:57)."""
+    return _predicate(IN_SPHERE_UNPERTURBED, points, idx)
+
+
+def coplanar_orientation(points, idx) -> np.ndarray:
+    """Rows of 3 (p,q,r) or 4 (p,q,r,s) indices (reference predicates2.h:33,40)."""
+    ix = np.asarray(idx)
+    kind = COPLANAR_ORIENTATION3 if ix.reshape(ix.shape[0], -1).shape[1] == 3 else COPLANAR_ORIENTATION4
+    return _predicate(kind, points, ix)
+
+
+def coplanar_in_circle(points, idx) -> np.ndarray:
+    """Perturbed in-circle per row (p0, p1, p2, p) (reference predicates2.h:66)."""
+    return _predicate(COPLANAR_IN_CIRCLE, points, idx)
+
+
+def coplanar_in_circle_unperturbed(points, idx) -> np.ndarray:
+    """Raw in-circle per row (reference predicates2.h:70)."""
+    return _predicate(COPLANAR_IN_CIRCLE_UNPERTURBED, points, idx)
+
+
+def collinear(points, idx) -> np.ndarray:
+    """1 where the row (p, q, r) is exactly collinear (reference predicates2.h:46)."""
+    return _predicate(COLLINEAR, points, idx)
+
+
+def orient2d(six) -> np.ndarray:
+    """Sign of |q-p, r-p| per row (px, py, qx, qy, rx, ry) (reference predicates2.h:27)."""
+    lib = library()
+    a = np.ascontiguousarray(six, dtype=np.float64).reshape(-1, 6)
+    out = np.zeros(a.shape[0], dtype=np.int8)
+    _check(lib.d3g_orient2d(_ptr(a), a.shape[0], _ptr(out)), "orient2d")
+    return out
+
+
+def spatial_sort(points, order: Optional[List[int]] = None) -> np.ndarray:
+    """The reference insertion order of `points` (reference spatial_sort.h:37).
+
+    As in the reference, `order` (if given) must be 0..n-1 on entry; it is
+    reordered in place when it is a list, and the order is also returned."""
+    lib = library()
+    pts = _points(points)
+    out = np.zeros(pts.shape[0], dtype=np.int32)
+    if pts.shape[0]:
+        _check(lib.d3g_spatial_sort(_ptr(pts), pts.shape[0], _ptr(out)), "spatial_sort")
+    if order is not None:
+        order[:] = out.tolist()
+    return out
+
+
+# ---- the build ------------------------------------------------------------------
+
+
+class Delaunay:
+    """The Delaunay triangulation of a point set (reference delaunay.h:62-92),
+    built on the GPU."""
+
+    def __init__(self) -> None:
+        self._cells = np.zeros((0, 4), dtype=np.int32)
+        self._all = np.zeros((0, 4), dtype=np.int32)
+        self._inc_off = np.zeros(1, dtype=np.int64)
+        self._inc = np.zeros(0, dtype=np.int32)
+        self._n_vertices = 0
+        self.rounds = 0
+        self.device_ms = 0.0
+
+    def build(self, points, chunk: int = 0) -> None:
+        """Builds the triangulation.  Points equal to an earlier point are
+        ignored; a repeated point is reported under the index of its copy that
+        comes last in the spatial-sort order, as in the reference."""
+        lib = library()
+        pts = _points(points)
+        opts = _Options()
+        lib.d3g_options_default(ctypes.byref(opts))
+        opts.chunk = int(chunk)
+        res = _Result()
+        _check(lib.d3g_build(_ptr(pts), pts.shape[0], ctypes.byref(opts), ctypes.byref(res)), "build")
+        try:
+            nc, na = res.n_cells, res.n_all
+            self._cells = (np.ctypeslib.as_array(res.cells, shape=(nc * 4,)).reshape(nc, 4).copy()
+                           if nc else np.zeros((0, 4), dtype=np.int32))
+            self._all = (np.ctypeslib.as_array(res.all_cells, shape=(na * 4,)).reshape(na, 4).copy()
+                         if na else np.zeros((0, 4), dtype=np.int32))
+            n = pts.shape[0]
+            self._inc_off = np.ctypeslib.as_array(res.incident_offsets, shape=(n + 1,)).copy()
+            ninc = int(self._inc_off[-1])
+            self._inc = (np.ctypeslib.as_array(res.incident, shape=(ninc,)).copy()
+                         if ninc else np.zeros(0, dtype=np.int32))
+            self._n_vertices = int(res.n_vertices)
+            self.rounds = int(res.rounds)
+            self.device_ms = float(res.device_ms)
+        finally:
+            lib.d3g_result_free(ctypes.byref(res))
+
+    def finite_cells(self) -> np.ndarray:
+        """(n_cells, 4) int32 finite tets, canonical order."""
+        return self._cells
+
+    def all_cells(self) -> np.ndarray:
+        """Every tet, infinite ones included (-1 = the infinite vertex), canonical order."""
+        return self._all
+
+    def incident_cells(self) -> List[np.ndarray]:
+        """Per input point, the ascending indices into finite_cells() of its cells."""
+        o = self._inc_off
+        return [self._inc[o[i]:o[i + 1]] for i in range(len(o) - 1)]
+
+    def incident_csr(self):
+        """incident_cells() as CSR arrays (offsets[n+1], indices)."""
+        return self._inc_off, self._inc
+
+    def number_of_vertices(self) -> int:
+        return self._n_vertices
+
+
+def build_device(points_dev, cap_cells: Optional[int] = None, stream: int = 0, chunk: int = 0):
+    """Builds from a device-resident torch tensor (n, 3) float64; returns the
+    canonical finite cells as a device int32 tensor (n_cells, 4) and the vertex
+    count.  Synchronises `stream`."""
+    import torch
+
+    lib = library()
+    assert points_dev.is_cuda and points_dev.dtype == torch.float64
+    x = points_dev.contiguous()
+    n = x.shape[0]
+    if cap_cells is None:
+        cap_cells = 8 * n + 64
+    out = torch.empty((cap_cells, 4), dtype=torch.int32, device=x.device)
+    nc, nv = _I64(0), _I64(0)
+    opts = _Options()
+    lib.d3g_options_default(ctypes.byref(opts))
+    opts.chunk = int(chunk)
+    _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), cap_cells,
+                                ctypes.byref(nc), ctypes.byref(nv), _P(stream)), "build_device")
+    return out[: nc.value], nv.value
+
+
+# ---- synthetic inputs -------------------------------------------------------------
+
+
+def gen_uniform(n: int, seed: int, lo: float = 0.0, hi: float = 1.0) -> np.ndarray:
+    """n points uniform in [lo, hi)^3 from std::mt19937(seed), u01 = word * 2^-32."""
+    out = np.zeros((n, 3), dtype=np.float64)
+    if n:
+        library().d3g_gen_uniform(n, seed, lo, hi, _ptr(out))
+    return out
+
+
+def gen_sphere(n: int, seed: int, r: float = 1.0, q: int = 1024, dedupe: bool = True) -> np.ndarray:
+    """Sphere samples snapped to a 1/q grid (duplicates removed, first kept)."""
+    out = np.zeros((n, 3), dtype=np.float64)
+    if n:
+        library().d3g_gen_sphere(n, seed, r, q, _ptr(out))
+    if dedupe and n:
+        _, first = np.unique(out, axis=0, return_index=True)
+        out = out[np.sort(first)]
+    return out
+
+
+def gen_clusters(n: int, seed: int, k: int = 8, sigma: float = 0.02) -> np.ndarray:
+    out = np.zeros((n, 3), dtype=np.float64)
+    if n:
+        library().d3g_gen_clusters(n, seed, k, sigma, _ptr(out))
+    return out
+
+
+def gen_lattice(n: int) -> np.ndarray:
+    out = np.zeros((n, 3), dtype=np.float64)
+    if n:
+        library().d3g_gen_lattice(n, _ptr(out))
+    return out

@@ -1,0 +1,1173 @@
+// The Delaunay build on the device: del3d::Delaunay::build
+// (src/triangulation.cpp:65-120, 702-769, 932-968) as parallel insertion rounds.
+//
+// Why a parallel build can return the reference's tets: in_sphere never
+// returns ZERO (symbolic perturbation, src/predicates.cpp:206-232) and the hull
+// conflict rule is fixed (src/triangulation.cpp:588-602), so the set of finite
+// cells is a function of the point set alone, whatever the insertion order.
+// The device therefore inserts many points at once, in rounds:
+//
+//   * Points are ordered by the spatial sort (sort.cu) and grouped into BRIO
+//     levels; each level is cut into chunks, one per worker.  A worker inserts
+//     its chunk's points one per round, so the points in flight in a round are
+//     spread along the Hilbert curve, i.e. far apart.
+//   * k_cavity   each worker walks from the last vertex it inserted to the tet
+//                its point conflicts with (visibility walk, exact orient3d),
+//                then grows the conflict region breadth-first with the
+//                reference's in_conflict rule, claiming every region tet and
+//                every tet across its boundary with a 64-bit atomicMin of
+//                (round, point rank) - the earliest point in insertion order
+//                wins ties.  A worker that meets a claim of an earlier point
+//                stops at once: it would lose anyway.
+//   * k_check    a worker wins if it still holds every claim.  Winners' regions
+//                and their one-ring of outside tets are pairwise disjoint, so
+//                winners can re-star concurrently without locks.
+//   * k_restar   each winner re-stars its region (one new tet per boundary
+//                facet, src/tds.h:160-221), reusing its region's slots, and
+//                advances to its next point.  The earliest pending point always
+//                wins, so every round makes progress.
+//
+// The output is canonicalised (even rotation, lexicographic sort), so it is
+// identical across runs whatever order the rounds happened to take.
+#include "device_util.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+namespace d3g {
+
+int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaStream_t s);
+int multiscale_bounds(int64_t n, int64_t* b, int cap);
+
+namespace {
+
+constexpr int kInf = -1;
+constexpr int kWalkLimit = 1 << 20;
+constexpr int kRotateLimit = 1 << 16;
+
+enum : int { WS_DONE = 0, WS_CAND = 1, WS_LOST = 2, WS_WIN = 3, WS_OVERFLOW = 4, WS_FAIL = 5 };
+
+__device__ __forceinline__ Pt vpt(const double* __restrict__ vx, int v) {
+    const double* p = vx + 3 * int64_t(v);
+    return Pt{p[0], p[1], p[2]};
+}
+
+__device__ __forceinline__ int at(const int4& t, int i) {
+    return i == 0 ? t.x : (i == 1 ? t.y : (i == 2 ? t.z : t.w));
+}
+__device__ __forceinline__ void set_at(int4& t, int i, int v) {
+    if (i == 0) t.x = v;
+    else if (i == 1) t.y = v;
+    else if (i == 2) t.z = v;
+    else t.w = v;
+}
+__device__ __forceinline__ int inf_pos(const int4& t) {
+    return t.x == kInf ? 0 : (t.y == kInf ? 1 : (t.z == kInf ? 2 : (t.w == kInf ? 3 : -1)));
+}
+__device__ __forceinline__ int pos_of(const int4& t, int v) {
+    return t.x == v ? 0 : (t.y == v ? 1 : (t.z == v ? 2 : 3));
+}
+
+struct Tables {
+    int4* tv;                  // vertices (kInf = the infinite vertex)
+    int4* tn;                  // neighbours: tet * 4 + the facet of that tet facing back
+    unsigned long long* claim; // per-round ownership claims
+    uint8_t* alive;
+    int* fnew;                 // per tet facet: the new tet built on it (restar scratch)
+    int* vert_tet;             // one live tet incident to each inserted vertex
+    int* tet_count;
+    int cap;
+};
+
+struct Workers {
+    int* cur;     // current point (vertex id) of each worker
+    int* beg;     // start of its chunk
+    int* end;     // end of its chunk
+    int* off;     // where in the chunk it started (chunks are walked cyclically)
+    int* done;    // points of its chunk handled so far
+    int* last;    // last vertex it inserted (-1: none yet)
+    int* guide;   // an inserted vertex near its chunk, for the first walk
+    int* state;
+    int* ncav;
+    int* nfac;
+    int* cav;     // worker-major scratch: cav_cap region tets per worker
+    int* fac;     // fac_cap boundary facets (tet * 4 + facet) per worker
+    int4* st_v;   // fac_cap staged new tets per worker (vertices) ...
+    int4* st_n;   // ... and neighbours
+    int cav_cap;
+    int fac_cap;
+    int n;
+};
+
+struct Round {
+    unsigned long long tag;   // (~round) << 32: newer rounds win every stale claim
+    int skip[4];              // the initial tet's vertices (already inserted)
+    int* counters;            // [0] active workers, [1] overflowed workers, [2] winners
+    uint32_t* status;
+};
+
+/// orient3d of tet (q0,q1,q2,q3) with vertex i replaced by p.
+__device__ __forceinline__ int orient_replaced(const Pt* q, int i, const Pt& p, uint32_t* st) {
+    switch (i) {
+        case 0: return orient3d(p, q[1], q[2], q[3], st);
+        case 1: return orient3d(q[0], p, q[2], q[3], st);
+        case 2: return orient3d(q[0], q[1], p, q[3], st);
+        default: return orient3d(q[0], q[1], q[2], p, st);
+    }
+}
+
+/// The reference's conflict test, src/triangulation.cpp:588-602.
+__device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __restrict__ vx,
+                            uint32_t* st) {
+    const int ip = inf_pos(t);
+    if (ip >= 0) {
+        // For each slot of the infinite vertex, the three finite vertices in
+        // the order that makes orient3d(a, b, d, p) the half-space test.
+        const int o0 = ip == 0 ? 2 : (ip == 1 ? 2 : (ip == 2 ? 1 : 0));
+        const int o1 = ip == 0 ? 1 : (ip == 1 ? 3 : (ip == 2 ? 0 : 1));
+        const int o2 = ip == 0 ? 3 : (ip == 1 ? 0 : (ip == 2 ? 3 : 2));
+        const int va = at(t, o0), vb = at(t, o1), vd = at(t, o2);
+        const Pt a = vpt(vx, va), b = vpt(vx, vb), d = vpt(vx, vd);
+        const int s = orient3d(a, b, d, p, st);
+        if (s != 0) return s > 0;
+        const int64_t id[4] = {va, vb, vd, pid};
+        return coplanar_in_circle(a, b, d, p, id, st) > 0;
+    }
+    const int64_t id[5] = {t.x, t.y, t.z, t.w, pid};
+    return in_sphere(vpt(vx, t.x), vpt(vx, t.y), vpt(vx, t.z), vpt(vx, t.w), p, id, st) > 0;
+}
+
+constexpr unsigned kFull = 0xffffffffu;
+
+/// Visibility walk from tet t to a tet in conflict with p: the finite tet
+/// containing p, or the infinite tet beyond the hull facet the walk crosses.
+/// Warp-cooperative: the four facet tests of a step run on lanes 0-3 and the
+/// first negative one in a pseudo-random cyclic order is crossed (never the
+/// facet just crossed).  Every lane returns the same tet.
+__device__ int walk_w(int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
+                      uint32_t* st, int lane) {
+    int4 tv = T.tv[t];
+    {
+        const int ip = inf_pos(tv);
+        if (ip >= 0) {
+            t = at(T.tn[t], ip) >> 2;
+            tv = T.tv[t];
+        }
+    }
+    int prev = -1;
+    uint32_t h = uint32_t(pid) * 2654435761u + 12345u;
+    for (int step = 0; step < kWalkLimit; ++step) {
+        const int4 tn = T.tn[t];
+        h = h * 1664525u + 1013904223u;
+        const int s0 = int(h >> 30);
+        bool neg = false;
+        if (lane < 4 && (at(tn, lane) >> 2) != prev) {
+            const Pt q[4] = {vpt(vx, tv.x), vpt(vx, tv.y), vpt(vx, tv.z), vpt(vx, tv.w)};
+            neg = orient_replaced(q, lane, p, st) < 0;
+        }
+        const unsigned m = __ballot_sync(kFull, neg) & 0xFu;
+        if (m == 0) return t;
+        const unsigned rot = ((m >> s0) | (m << (4 - s0))) & 0xFu;
+        const int i = (s0 + __ffs(int(rot)) - 1) & 3;
+        const int next = at(tn, i) >> 2;
+        const int4 nv = T.tv[next];
+        if (inf_pos(nv) >= 0) return next;
+        prev = t;
+        t = next;
+        tv = nv;
+    }
+    report(st, ST_WALK_LIMIT);
+    return -1;
+}
+
+/// Advances worker w to the next point of its chunk (walked cyclically from its
+/// start offset), skipping the initial tet's vertices; -1 when the chunk is done.
+__device__ int next_point(const Workers& W, int w, const int* skip) {
+    const int b = W.beg[w], len = W.end[w] - b, off = W.off[w];
+    int done = W.done[w];
+    int v = -1;
+    while (done < len) {
+        const int c = b + (off + done) % len;
+        ++done;
+        if (c != skip[0] && c != skip[1] && c != skip[2] && c != skip[3]) {
+            v = c;
+            break;
+        }
+    }
+    W.done[w] = done;
+    W.cur[w] = v;
+    return v;
+}
+
+/// One warp per worker: locate the worker's point, then grow its conflict
+/// region breadth-first, eight region tets (32 facets) per step, claiming
+/// every region tet (key) and every tet across the region boundary (key|1).
+__global__ void __launch_bounds__(128) k_cavity(Tables T, Workers W, Round R, const double* __restrict__ vx,
+                                                int first) {
+    const int lane = threadIdx.x & 31;
+    const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (w >= W.n) return;
+    const int v = W.cur[w];
+    if (v < 0) {
+        if (lane == 0) W.state[w] = WS_DONE;
+        return;
+    }
+    const Pt p = vpt(vx, v);
+    const int sv = W.last[w] >= 0 ? W.last[w] : W.guide[w];
+    const int seed = walk_w(T.vert_tet[sv], p, v, T, vx, R.status, lane);
+    if (seed < 0) {
+        if (lane == 0) W.state[w] = WS_FAIL;
+        return;
+    }
+    const unsigned long long key = R.tag | (unsigned long long)(uint32_t(v)) << 1;
+    const unsigned long long mine = key >> 1;
+    int* cav = W.cav + int64_t(w) * W.cav_cap;
+    int* fac = W.fac + int64_t(w) * W.fac_cap;
+    int lost = 0;
+    if (lane == 0) {
+        const unsigned long long old = atomicMin(T.claim + seed, key);
+        lost = (old >> 1) < mine;
+        cav[0] = seed;
+    }
+    if (__shfl_sync(kFull, lost, 0)) {
+        if (lane == 0) W.state[w] = WS_LOST;
+        return;
+    }
+    __syncwarp();
+    const unsigned lt = (1u << lane) - 1u;
+    int ncav = 1, nfac = 0, head = 0;
+    while (head < ncav) {
+        const int nproc = min(ncav - head, 8);
+        const bool valid = (lane >> 2) < nproc;
+        const int i = lane & 3;
+        int c = 0, nb = 0;
+        int kind = 0;   // 0: nothing, 1: boundary facet, 2: new region tet, 3: re-check
+        bool abort = false;
+        if (valid) {
+            c = cav[head + (lane >> 2)];
+            nb = at(T.tn[c], i) >> 2;
+            const unsigned long long old = atomicMin(T.claim + nb, key | 1ull);
+            if (old == key) {
+                kind = 0;                               // already in the region
+            } else if (old == (key | 1ull)) {
+                kind = 3;                               // seen by us: decided below
+            } else if ((old >> 1) < mine) {
+                abort = true;                           // an earlier point holds it
+            } else if (in_conflict(T.tv[nb], p, v, vx, R.status)) {
+                const unsigned long long o2 = atomicMin(T.claim + nb, key);
+                if ((o2 >> 1) < mine) abort = true;
+                else kind = 2;
+            } else {
+                kind = 1;
+            }
+        }
+        if (__any_sync(kFull, abort)) {
+            if (lane == 0) W.state[w] = WS_LOST;
+            return;
+        }
+        __syncwarp();
+        if (kind == 3) {
+            // Another lane of this step may have just turned it into a region tet.
+            const unsigned long long now = __ldcg(T.claim + nb);
+            if (now == key) kind = 0;
+            else if ((now >> 1) < mine) abort = true;
+            else kind = 1;
+        }
+        if (__any_sync(kFull, abort)) {
+            if (lane == 0) W.state[w] = WS_LOST;
+            return;
+        }
+        const unsigned mc = __ballot_sync(kFull, kind == 2);
+        const unsigned mf = __ballot_sync(kFull, kind == 1);
+        if (ncav + __popc(mc) > W.cav_cap || nfac + __popc(mf) > W.fac_cap) {
+            if (lane == 0) {
+                W.state[w] = WS_OVERFLOW;
+                atomicAdd(R.counters + 1, 1);
+            }
+            return;
+        }
+        if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
+        if (kind == 1) fac[nfac + __popc(mf & lt)] = c * 4 + i;
+        ncav += __popc(mc);
+        nfac += __popc(mf);
+        head += nproc;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        W.ncav[w] = ncav;
+        W.nfac[w] = nfac;
+        W.state[w] = WS_CAND;
+    }
+}
+
+/// One warp per candidate: it wins if it still holds every claim it made.
+__global__ void __launch_bounds__(128) k_check(Tables T, Workers W, Round R, int first) {
+    const int lane = threadIdx.x & 31;
+    const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (w >= W.n || W.state[w] != WS_CAND) return;
+    const int v = W.cur[w];
+    const unsigned long long key = R.tag | (unsigned long long)(uint32_t(v)) << 1;
+    const int* cav = W.cav + int64_t(w) * W.cav_cap;
+    const int* fac = W.fac + int64_t(w) * W.fac_cap;
+    const int ncav = W.ncav[w], nfac = W.nfac[w];
+    bool ok = true;
+    for (int k = lane; k < ncav; k += 32) ok = ok && T.claim[cav[k]] == key;
+    for (int k = lane; k < nfac; k += 32) {
+        const int f = fac[k];
+        ok = ok && T.claim[at(T.tn[f >> 2], f & 3) >> 2] == (key | 1ull);
+    }
+    const bool win = __all_sync(kFull, ok);
+    if (lane == 0) W.state[w] = win ? WS_WIN : WS_LOST;
+}
+
+/// One warp per winner: re-star its region, one boundary facet per lane.
+__global__ void __launch_bounds__(128) k_restar(Tables T, Workers W, Round R, int first) {
+    __shared__ int sh_count[2];
+    const int lane = threadIdx.x & 31;
+    const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (threadIdx.x < 2) sh_count[threadIdx.x] = 0;
+    __syncthreads();
+    const bool exists = w < W.n;
+    const int state = exists ? W.state[w] : WS_DONE;
+    const int v = exists ? W.cur[w] : -1;
+    bool advanced = false;
+    if (state == WS_WIN) {
+        const unsigned long long key = R.tag | (unsigned long long)(uint32_t(v)) << 1;
+        const int* cav = W.cav + int64_t(w) * W.cav_cap;
+        const int* fac = W.fac + int64_t(w) * W.fac_cap;
+        int4* sv = W.st_v + int64_t(w) * W.fac_cap;
+        int4* sn = W.st_n + int64_t(w) * W.fac_cap;
+        const int C = W.ncav[w], F = W.nfac[w];
+        const int extra = F > C ? F - C : 0;
+        int base = 0, ok = 1;
+        if (lane == 0 && extra > 0) {
+            base = atomicAdd(T.tet_count, extra);
+            if (base + extra > T.cap) {
+                report(R.status, ST_TET_CAPACITY);
+                ok = 0;
+            }
+        }
+        base = __shfl_sync(kFull, base, 0);
+        ok = __shfl_sync(kFull, ok, 0);
+        if (ok) {
+            // 1a: the new tet of each boundary facet.
+            for (int k = lane; k < F; k += 32) T.fnew[fac[k]] = k < C ? cav[k] : base + (k - C);
+            __syncwarp();
+            // 1b: vertices and neighbours, from the region as it was.
+            bool bad = false;
+            for (int k = lane; k < F && !bad; k += 32) {
+                const int c = fac[k] >> 2, i = fac[k] & 3;
+                const int4 cv = T.tv[c];
+                const int4 cn = T.tn[c];
+                int4 nv = cv, nn = cn;
+                set_at(nv, i, v);
+                for (int j = 0; j < 4 && !bad; ++j) {
+                    if (j == i) continue;
+                    // Facet j of the new tet is {v} + edge (va, vb); its neighbour is
+                    // the new tet on the other boundary facet through that edge,
+                    // reached by turning around the edge inside the region.
+                    int a = -1, b = -1;
+                    for (int m = 0; m < 4; ++m)
+                        if (m != i && m != j) {
+                            if (a < 0) a = m;
+                            else b = m;
+                        }
+                    const int va = at(cv, a), vb = at(cv, b);
+                    int cur = c, f = j, steps = 0;
+                    for (;;) {
+                        const int enc = at(T.tn[cur], f);
+                        const int nb = enc >> 2;
+                        if (T.claim[nb] != key) {   // (cur, f) is a boundary facet
+                            const int4 tc = T.tv[cur];
+                            const int wpos = 6 - f - pos_of(tc, va) - pos_of(tc, vb);
+                            if (wpos < 0 || wpos > 3 || wpos == f) bad = true;
+                            else set_at(nn, j, T.fnew[cur * 4 + f] * 4 + wpos);
+                            break;
+                        }
+                        const int4 tb = T.tv[nb];
+                        const int g = enc & 3;
+                        f = 6 - g - pos_of(tb, va) - pos_of(tb, vb);
+                        cur = nb;
+                        if (f < 0 || f > 3 || f == g || ++steps > kRotateLimit) {
+                            bad = true;
+                            break;
+                        }
+                    }
+                }
+                sv[k] = nv;
+                sn[k] = nn;
+            }
+            if (__any_sync(kFull, bad)) {
+                if (lane == 0) report(R.status, ST_INTERNAL);
+                ok = 0;
+            }
+            __syncwarp();
+        }
+        if (ok) {
+            // 2: write the new tets and re-point the outside neighbours.
+            for (int k = lane; k < F; k += 32) {
+                const int id = k < C ? cav[k] : base + (k - C);
+                const int4 nv = sv[k], nn = sn[k];
+                const int i = fac[k] & 3;
+                T.tv[id] = nv;
+                T.tn[id] = nn;
+                T.alive[id] = 1;
+                const int enc = at(nn, i);
+                reinterpret_cast<int*>(T.tn)[(enc >> 2) * 4 + (enc & 3)] = id * 4 + i;
+                if (nv.x != kInf) T.vert_tet[nv.x] = id;
+                if (nv.y != kInf) T.vert_tet[nv.y] = id;
+                if (nv.z != kInf) T.vert_tet[nv.z] = id;
+                if (nv.w != kInf) T.vert_tet[nv.w] = id;
+            }
+            for (int k = F + lane; k < C; k += 32) T.alive[cav[k]] = 0;
+            advanced = true;
+        }
+    }
+    if (lane == 0 && exists) {
+        int cur = v;
+        if (advanced) {
+            W.last[w] = v;
+            cur = next_point(W, w, R.skip);
+        }
+        if (state != WS_DONE && cur >= 0) atomicAdd(sh_count, 1);
+        if (advanced) atomicAdd(sh_count + 1, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (sh_count[0]) atomicAdd(R.counters, sh_count[0]);
+        if (sh_count[1]) atomicAdd(R.counters + 2, sh_count[1]);
+    }
+}
+
+/// Workers of one level [lb, le): one chunk each.  Each starts at a scattered
+/// offset inside its chunk: chunks that are neighbours along the curve are
+/// mirror images of each other, and workers walking them in step would reach
+/// their common boundary together and keep colliding.
+__global__ void k_setup_level(Workers W, int lb, int le, int chunk, int plb, int ple, int4 skip4) {
+    const int w = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (w >= W.n) return;
+    const int b = lb + w * chunk;
+    const int e = min(le, b + chunk);
+    const int len = e - b;
+    const int off = len > 0 ? int((uint32_t(w) * 2654435761u >> 7) % uint32_t(len)) : 0;
+    W.beg[w] = b;
+    W.end[w] = e;
+    W.off[w] = off;
+    W.done[w] = 0;
+    W.last[w] = -1;
+    const int skip[4] = {skip4.x, skip4.y, skip4.z, skip4.w};
+    next_point(W, w, skip);
+    // The previous level is ordered along the same curve: the same fraction
+    // along it lands near this worker's first point.
+    int g = skip4.x;
+    if (ple > plb) {
+        const double frac = (double(w) * chunk + off) / double(le - lb);
+        g = plb + int(frac * double(ple - plb));
+        if (g >= ple) g = ple - 1;
+    }
+    W.guide[w] = g;
+    W.state[w] = WS_DONE;
+}
+
+// ---- set-up: validation, duplicates, initial tet ----------------------------------
+
+__global__ void k_check_finite(const double* __restrict__ xyz, int64_t n3, uint32_t* bad) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n3;
+         i += int64_t(gridDim.x) * blockDim.x)
+        if (!isfinite(xyz[i])) atomicOr(bad, 1u);
+}
+
+/// Coordinate bit patterns (with -0.0 folded onto +0.0, which compare equal)
+/// of the point at each rank, for the duplicate grouping.
+__global__ void k_coord_keys(const double* __restrict__ xyz, const int32_t* __restrict__ order,
+                             int64_t n, int axis, unsigned long long* __restrict__ keys,
+                             const int32_t* __restrict__ ranks) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const double x = xyz[3 * int64_t(order[ranks[i]]) + axis];
+        keys[i] = x == 0.0 ? 0ull : (unsigned long long)__double_as_longlong(x);
+    }
+}
+
+__device__ __forceinline__ bool same_point(const double* xyz, int32_t i, int32_t j) {
+    const double* a = xyz + 3 * int64_t(i);
+    const double* b = xyz + 3 * int64_t(j);
+    return a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
+}
+
+/// Over ranks sorted by coordinates (ties by rank): flags the first rank of
+/// each group of equal points and records the group's representative, the
+/// point with the LAST rank (src/triangulation.cpp:77-81).
+__global__ void k_groups(const double* __restrict__ xyz, const int32_t* __restrict__ order,
+                         const int32_t* __restrict__ sranks, int64_t n, int32_t* __restrict__ first,
+                         int32_t* __restrict__ rep_at_first, int* ndup) {
+    for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < n;
+         s += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t r = sranks[s];
+        const bool starts = s == 0 || !same_point(xyz, order[sranks[s - 1]], order[r]);
+        if (!starts) {
+            first[r] = 0;
+            atomicAdd(ndup, 1);
+            continue;
+        }
+        int64_t e = s;
+        while (e + 1 < n && same_point(xyz, order[sranks[e + 1]], order[r])) ++e;
+        first[r] = 1;
+        rep_at_first[r] = order[sranks[e]];
+    }
+}
+
+__global__ void k_vertices(const double* __restrict__ xyz, const int32_t* __restrict__ order,
+                           const int32_t* __restrict__ first, const int32_t* __restrict__ vid_of_rank,
+                           const int32_t* __restrict__ rep_at_first, int64_t n, bool dups,
+                           double* __restrict__ vx, int32_t* __restrict__ vert_point) {
+    for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+         r += int64_t(gridDim.x) * blockDim.x) {
+        if (dups && !first[r]) continue;
+        const int32_t v = dups ? vid_of_rank[r] : int32_t(r);
+        const int32_t i = order[r];
+        vx[3 * int64_t(v)] = xyz[3 * int64_t(i)];
+        vx[3 * int64_t(v) + 1] = xyz[3 * int64_t(i) + 1];
+        vx[3 * int64_t(v) + 2] = xyz[3 * int64_t(i) + 2];
+        vert_point[v] = dups ? rep_at_first[r] : i;
+    }
+}
+
+__global__ void k_find_noncollinear(const double* __restrict__ vx, int nv, int* found, uint32_t* st) {
+    const Pt a = vpt(vx, 0), b = vpt(vx, 1);
+    for (int v = 2 + int(blockIdx.x) * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        if (v > *found) return;
+        if (!collinear(a, b, vpt(vx, v), st)) atomicMin(found, v);
+    }
+}
+
+__global__ void k_find_noncoplanar(const double* __restrict__ vx, int nv, int v2, int* found,
+                                   uint32_t* st) {
+    const Pt a = vpt(vx, 0), b = vpt(vx, 1), c = vpt(vx, v2);
+    for (int v = 2 + int(blockIdx.x) * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        if (v > *found) return;
+        if (v != v2 && orient3d(a, b, c, vpt(vx, v), st) != 0) atomicMin(found, v);
+    }
+}
+
+/// One thread: the first tet and its four infinite neighbours.
+__global__ void k_init_tets(Tables T, const double* __restrict__ vx, int v0, int v1, int v2, int v3,
+                            uint32_t* st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (orient3d(vpt(vx, v0), vpt(vx, v1), vpt(vx, v2), vpt(vx, v3), st) < 0) {
+        const int t = v0;
+        v0 = v1;
+        v1 = t;
+    }
+    int4 tv[5];
+    tv[0] = make_int4(v0, v1, v2, v3);
+    for (int i = 0; i < 4; ++i) {
+        // Facet i of the first tet, capped by the infinite vertex in slot i and
+        // two other slots swapped, so the cap is positively oriented.
+        int4 c = tv[0];
+        set_at(c, i, kInf);
+        const int a = (i + 1) & 3, b = (i + 2) & 3;
+        const int x = at(c, a);
+        set_at(c, a, at(c, b));
+        set_at(c, b, x);
+        tv[1 + i] = c;
+    }
+    int4 tn[5];
+    for (int t = 0; t < 5; ++t)
+        for (int f = 0; f < 4; ++f) {
+            int fv[3], w = 0;
+            for (int m = 0; m < 4; ++m)
+                if (m != f) fv[w++] = at(tv[t], m);
+            for (int u = 0; u < 5; ++u) {
+                if (u == t) continue;
+                for (int g = 0; g < 4; ++g) {
+                    int hits = 0;
+                    for (int m = 0; m < 4; ++m) {
+                        if (m == g) continue;
+                        const int x = at(tv[u], m);
+                        hits += (x == fv[0]) + (x == fv[1]) + (x == fv[2]);
+                    }
+                    if (hits == 3) set_at(tn[t], f, u * 4 + g);
+                }
+            }
+        }
+    for (int t = 0; t < 5; ++t) {
+        T.tv[t] = tv[t];
+        T.tn[t] = tn[t];
+        T.alive[t] = 1;
+    }
+    T.vert_tet[v0] = 0;
+    T.vert_tet[v1] = 0;
+    T.vert_tet[v2] = 0;
+    T.vert_tet[v3] = 0;
+    *T.tet_count = 5;
+}
+
+// ---- output -----------------------------------------------------------------------
+
+/// Even permutation bringing the smallest index to slot 0, then the cyclic
+/// rotation of the other three that puts their smallest first.
+__device__ __forceinline__ int4 canonical(int4 t) {
+    int m = 0;
+    int mv = t.x;
+    if (t.y < mv) { m = 1; mv = t.y; }
+    if (t.z < mv) { m = 2; mv = t.z; }
+    if (t.w < mv) { m = 3; mv = t.w; }
+    if (m == 1) t = make_int4(t.y, t.x, t.w, t.z);
+    else if (m == 2) t = make_int4(t.z, t.w, t.x, t.y);
+    else if (m == 3) t = make_int4(t.w, t.z, t.y, t.x);
+    if (t.z < t.y && t.z < t.w) t = make_int4(t.x, t.z, t.w, t.y);
+    else if (t.w < t.y && t.w < t.z) t = make_int4(t.x, t.w, t.y, t.z);
+    return t;
+}
+
+__global__ void k_cell_flags(const int4* __restrict__ tv, const uint8_t* __restrict__ alive, int ntet,
+                             bool with_infinite, int32_t* __restrict__ flag) {
+    for (int t = int(blockIdx.x) * blockDim.x + threadIdx.x; t < ntet; t += gridDim.x * blockDim.x) {
+        const int4 c = tv[t];
+        flag[t] = alive[t] && (with_infinite || inf_pos(c) < 0) ? 1 : 0;
+    }
+}
+
+/// Writes the flagged tets, mapped to input point indices and canonicalised,
+/// plus their sort keys (shifted by one so the infinite vertex, -1, is 0).
+__global__ void k_cells_out(const int4* __restrict__ tv, const int32_t* __restrict__ flag,
+                            const int32_t* __restrict__ pos, int ntet,
+                            const int32_t* __restrict__ vert_point, int kbits, int4* __restrict__ cells,
+                            unsigned long long* __restrict__ khi, unsigned long long* __restrict__ klo,
+                            int32_t* __restrict__ idx) {
+    for (int t = int(blockIdx.x) * blockDim.x + threadIdx.x; t < ntet; t += gridDim.x * blockDim.x) {
+        if (!flag[t]) continue;
+        const int4 c = tv[t];
+        int4 q;
+        q.x = c.x == kInf ? -1 : vert_point[c.x];
+        q.y = c.y == kInf ? -1 : vert_point[c.y];
+        q.z = c.z == kInf ? -1 : vert_point[c.z];
+        q.w = c.w == kInf ? -1 : vert_point[c.w];
+        q = canonical(q);
+        const int o = pos[t];
+        cells[o] = q;
+        khi[o] = ((unsigned long long)(uint32_t(q.x + 1)) << kbits) | uint32_t(q.y + 1);
+        klo[o] = ((unsigned long long)(uint32_t(q.z + 1)) << kbits) | uint32_t(q.w + 1);
+        idx[o] = o;
+    }
+}
+
+__global__ void k_gather_cells(const int4* __restrict__ in, const int32_t* __restrict__ idx, int64_t n,
+                               int4* __restrict__ out) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = in[idx[i]];
+}
+
+__global__ void k_incident_pairs(const int4* __restrict__ cells, int64_t nc, int32_t* __restrict__ pt,
+                                 int32_t* __restrict__ cell, int32_t* __restrict__ count) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nc;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const int4 c = cells[i];
+        const int v[4] = {c.x, c.y, c.z, c.w};
+        for (int k = 0; k < 4; ++k) {
+            pt[4 * i + k] = v[k];
+            cell[4 * i + k] = int32_t(i);
+            atomicAdd(count + v[k], 1);
+        }
+    }
+}
+
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
+__global__ void k_gather_u64(const unsigned long long* __restrict__ in, const int32_t* __restrict__ ix,
+                             int64_t m, unsigned long long* __restrict__ o) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += int64_t(gridDim.x) * blockDim.x)
+        o[i] = in[ix[i]];
+}
+
+__global__ void k_iota32(int32_t* __restrict__ a, int64_t m) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += int64_t(gridDim.x) * blockDim.x)
+        a[i] = int32_t(i);
+}
+
+__global__ void k_widen(const int32_t* __restrict__ a, int64_t m, int64_t* __restrict__ o) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += int64_t(gridDim.x) * blockDim.x)
+        o[i] = a[i];
+}
+
+}  // namespace
+
+/// Device-resident result of one build.
+struct DeviceResult {
+    DevBuf<int4> cells;
+    DevBuf<int4> all;
+    DevBuf<int64_t> inc_off;
+    DevBuf<int32_t> inc;
+    int64_t n_cells = 0, n_all = 0, n_vertices = 0, n_inc = 0;
+    int rounds = 0;
+    void reset() {
+        cells.release();
+        all.release();
+        inc_off.release();
+        inc.release();
+        n_cells = n_all = n_vertices = n_inc = 0;
+        rounds = 0;
+    }
+};
+
+namespace {
+
+/// Sorts `n` canonical cells lexicographically into `out` (keys prepared by
+/// k_cells_out).
+int sort_cells(DevBuf<int4>& cells, DevBuf<unsigned long long>& khi, DevBuf<unsigned long long>& klo,
+               DevBuf<int32_t>& idx, int64_t n, int kbits, DevBuf<int4>& out, cudaStream_t s) {
+    D3G_TRY(out.alloc(size_t(n), s));
+    if (n == 0) return D3G_OK;
+    DevBuf<unsigned long long> k2;
+    DevBuf<int32_t> i2;
+    D3G_TRY(k2.alloc(size_t(n), s));
+    D3G_TRY(i2.alloc(size_t(n), s));
+    // LSD: low half first, then a stable sort on the high half.
+    D3G_TRY(sort_pairs(klo.p, k2.p, idx.p, i2.p, n, 0, 2 * kbits, s));
+    // Re-gather the high keys in that order, then sort by them.
+    DevBuf<unsigned long long> khi2;
+    D3G_TRY(khi2.alloc(size_t(n), s));
+    k_gather_u64<<<grid_for(n, 256), 256, 0, s>>>(khi.p, i2.p, n, khi2.p);
+    D3G_TRY(sort_pairs(khi2.p, k2.p, i2.p, idx.p, n, 0, 2 * kbits, s));
+    k_gather_cells<<<grid_for(n, 256), 256, 0, s>>>(cells.p, idx.p, n, out.p);
+    D3G_CUDA(cudaGetLastError());
+    return D3G_OK;
+}
+
+}  // namespace
+
+int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
+                      DeviceResult& R) {
+    R.reset();
+    if (n == 0) return D3G_OK;
+    if (n > (int64_t(1) << 27)) {
+        set_error("d3g_build: at most 2^27 points per set");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    const int N = int(n);
+    DevBuf<uint32_t> status;
+    D3G_TRY(status.alloc(4, s));
+    D3G_CUDA(cudaMemsetAsync(status.p, 0, 4 * sizeof(uint32_t), s));
+    k_check_finite<<<grid_for(3 * n, 256), 256, 0, s>>>(d_xyz, 3 * n, status.p + 1);
+
+    // ---- insertion order and duplicate groups ----
+    DevBuf<int32_t> order;
+    D3G_TRY(order.alloc(size_t(N), s));
+    D3G_TRY(spatial_order_device(d_xyz, n, order.p, s));
+
+    DevBuf<double> vx;
+    DevBuf<int32_t> vert_point;
+    int nv = N;
+    {
+        DevBuf<int32_t> ranks, sranks, first, rep, vid;
+        DevBuf<unsigned long long> keys, keys2;
+        DevBuf<int> ndup;
+        D3G_TRY(ranks.alloc(size_t(N), s));
+        D3G_TRY(sranks.alloc(size_t(N), s));
+        D3G_TRY(keys.alloc(size_t(N), s));
+        D3G_TRY(keys2.alloc(size_t(N), s));
+        D3G_TRY(ndup.alloc(1, s));
+        D3G_CUDA(cudaMemsetAsync(ndup.p, 0, sizeof(int), s));
+        k_iota32<<<grid_for(n, 256), 256, 0, s>>>(ranks.p, n);
+        // LSD over z, y, x: ranks sorted by coordinates, ties kept in rank order.
+        for (int axis = 2; axis >= 0; --axis) {
+            k_coord_keys<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, n, axis, keys.p, ranks.p);
+            D3G_TRY(sort_pairs(keys.p, keys2.p, ranks.p, sranks.p, n, 0, 64, s));
+            std::swap(ranks.p, sranks.p);
+        }
+        D3G_TRY(first.alloc(size_t(N), s));
+        D3G_TRY(rep.alloc(size_t(N), s));
+        k_groups<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, ranks.p, n, first.p, rep.p, ndup.p);
+        int hdup = 0;
+        D3G_CUDA(cudaMemcpyAsync(&hdup, ndup.p, sizeof hdup, cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));
+        nv = N - hdup;
+        D3G_TRY(vx.alloc(size_t(3) * nv, s));
+        D3G_TRY(vert_point.alloc(size_t(nv), s));
+        if (hdup > 0) {
+            D3G_TRY(vid.alloc(size_t(N), s));
+            D3G_TRY(exclusive_scan(first.p, vid.p, n, s));
+        }
+        k_vertices<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, first.p, vid.p, rep.p, n, hdup > 0,
+                                                    vx.p, vert_point.p);
+        D3G_CUDA(cudaGetLastError());
+    }
+    order.release();
+    R.n_vertices = nv;
+
+    uint32_t hst[2] = {0, 0};
+    D3G_CUDA(cudaMemcpyAsync(hst, status.p, sizeof hst, cudaMemcpyDeviceToHost, s));
+    D3G_CUDA(cudaStreamSynchronize(s));
+    if (hst[1]) {
+        set_error("d3g_build: non-finite coordinate");
+        return D3G_ERR_INVALID_INPUT;
+    }
+
+    // ---- the first tet: the first four affinely independent vertices ----
+    int v2 = -1, v3 = -1;
+    if (nv >= 4) {
+        DevBuf<int> found;
+        D3G_TRY(found.alloc(2, s));
+        k_set_int<<<1, 1, 0, s>>>(found.p, nv);
+        k_set_int<<<1, 1, 0, s>>>(found.p + 1, nv);
+        k_find_noncollinear<<<grid_for(nv, 256), 256, 0, s>>>(vx.p, nv, found.p, status.p);
+        int h = nv;
+        D3G_CUDA(cudaMemcpyAsync(&h, found.p, sizeof h, cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));
+        if (h < nv) {
+            v2 = h;
+            k_find_noncoplanar<<<grid_for(nv, 256), 256, 0, s>>>(vx.p, nv, v2, found.p + 1, status.p);
+            D3G_CUDA(cudaMemcpyAsync(&h, found.p + 1, sizeof h, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaStreamSynchronize(s));
+            if (h < nv) v3 = h;
+        }
+    }
+    if (v3 < 0) {
+        // Every point collinear or coplanar: no cells (src/triangulation.cpp:943-949).
+        D3G_CUDA(cudaMemcpyAsync(hst, status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));
+        const int st = status_from_bits(hst[0]);
+        if (st != D3G_OK) return st;
+        if (opt.want_incident) {
+            D3G_TRY(R.inc_off.alloc(size_t(N) + 1, s));
+            D3G_CUDA(cudaMemsetAsync(R.inc_off.p, 0, sizeof(int64_t) * (size_t(N) + 1), s));
+        }
+        return D3G_OK;
+    }
+
+    // ---- tables ----
+    Tables T;
+    int64_t cap64 = int64_t(nv) * 8 + 4096;
+    if (cap64 > (int64_t(1) << 29)) cap64 = int64_t(1) << 29;
+    T.cap = int(cap64);
+    DevBuf<int4> tv, tn;
+    DevBuf<unsigned long long> claim;
+    DevBuf<uint8_t> alive;
+    DevBuf<int> fnew, vert_tet, tet_count;
+    D3G_TRY(tv.alloc(size_t(T.cap), s));
+    D3G_TRY(tn.alloc(size_t(T.cap), s));
+    D3G_TRY(claim.alloc(size_t(T.cap), s));
+    D3G_TRY(alive.alloc(size_t(T.cap), s));
+    D3G_TRY(fnew.alloc(size_t(T.cap) * 4, s));
+    D3G_TRY(vert_tet.alloc(size_t(nv), s));
+    D3G_TRY(tet_count.alloc(1, s));
+    D3G_CUDA(cudaMemsetAsync(claim.p, 0xFF, sizeof(unsigned long long) * size_t(T.cap), s));
+    D3G_CUDA(cudaMemsetAsync(alive.p, 0, size_t(T.cap), s));
+    T.tv = tv.p;
+    T.tn = tn.p;
+    T.claim = claim.p;
+    T.alive = alive.p;
+    T.fnew = fnew.p;
+    T.vert_tet = vert_tet.p;
+    T.tet_count = tet_count.p;
+    k_init_tets<<<1, 32, 0, s>>>(T, vx.p, 0, 1, v2, v3, status.p);
+
+    // ---- workers ----
+    const int chunk = opt.chunk > 0 ? opt.chunk : 64;
+    int64_t hb[64];
+    const int nb = multiscale_bounds(nv, hb, 63);
+    int maxw = 1;
+    for (int k = 0; k < nb; ++k) {
+        const int64_t lo = (k + 1 < nb) ? hb[k + 1] : 0;
+        const int64_t cnt = hb[k] - lo;
+        maxw = std::max<int64_t>(maxw, (cnt + chunk - 1) / chunk);
+    }
+    Workers W;
+    W.cav_cap = 256;
+    W.fac_cap = 512;
+    W.n = maxw;
+    DevBuf<int> wcur, wbeg, wend, woff, wdone, wlast, wguide, wstate, wncav, wnfac, wcav, wfac, counters;
+    DevBuf<int4> wsv, wsn;
+    D3G_TRY(wcur.alloc(size_t(maxw), s));
+    D3G_TRY(wend.alloc(size_t(maxw), s));
+    D3G_TRY(wbeg.alloc(size_t(maxw), s));
+    D3G_TRY(woff.alloc(size_t(maxw), s));
+    D3G_TRY(wdone.alloc(size_t(maxw), s));
+    D3G_TRY(wlast.alloc(size_t(maxw), s));
+    D3G_TRY(wguide.alloc(size_t(maxw), s));
+    D3G_TRY(wstate.alloc(size_t(maxw), s));
+    D3G_TRY(wncav.alloc(size_t(maxw), s));
+    D3G_TRY(wnfac.alloc(size_t(maxw), s));
+    D3G_TRY(wcav.alloc(size_t(maxw) * W.cav_cap, s));
+    D3G_TRY(wfac.alloc(size_t(maxw) * W.fac_cap, s));
+    D3G_TRY(wsv.alloc(size_t(maxw) * W.fac_cap, s));
+    D3G_TRY(wsn.alloc(size_t(maxw) * W.fac_cap, s));
+    D3G_TRY(counters.alloc(3, s));
+    W.cur = wcur.p;
+    W.end = wend.p;
+    W.beg = wbeg.p;
+    W.off = woff.p;
+    W.done = wdone.p;
+    W.last = wlast.p;
+    W.guide = wguide.p;
+    W.state = wstate.p;
+    W.ncav = wncav.p;
+    W.nfac = wnfac.p;
+    W.cav = wcav.p;
+    W.fac = wfac.p;
+    W.st_v = wsv.p;
+    W.st_n = wsn.p;
+
+    Round Rd;
+    Rd.skip[0] = 0;
+    Rd.skip[1] = 1;
+    Rd.skip[2] = v2;
+    Rd.skip[3] = v3;
+    Rd.counters = counters.p;
+    Rd.status = status.p;
+    const int max_rounds = opt.max_rounds > 0 ? opt.max_rounds : (1 << 20);
+    int round = 0;
+    const bool trace = getenv("D3G_TRACE") != nullptr;
+    // Levels from the coarsest ([0, hb[nb-1])) to the finest ([hb[1], hb[0])).
+    for (int k = nb - 1; k >= 0; --k) {
+        const int lb = int(k + 1 < nb ? hb[k + 1] : 0);
+        const int le = int(hb[k]);
+        const int plb = int(k + 2 < nb ? hb[k + 2] : 0);
+        const int ple = lb;
+        if (le <= lb) continue;
+        W.n = (le - lb + chunk - 1) / chunk;
+        const int round0 = round;
+        long long won = 0, attempts = 0;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        if (trace) {
+            cudaEventCreate(&ev0);
+            cudaEventCreate(&ev1);
+            cudaEventRecord(ev0, s);
+        }
+        k_setup_level<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, lb, le, chunk, plb, ple,
+                                                                  make_int4(0, 1, v2, v3));
+        for (;;) {
+            if (++round > max_rounds) {
+                set_error("d3g_build: insertion round limit reached");
+                return D3G_ERR_ROUND_LIMIT;
+            }
+            Rd.tag = (unsigned long long)(0xFFFFFFFFu - uint32_t(round)) << 32;
+            D3G_CUDA(cudaMemsetAsync(counters.p, 0, 3 * sizeof(int), s));
+            const unsigned g = unsigned((int64_t(W.n) * 32 + 127) / 128);
+            k_cavity<<<g, 128, 0, s>>>(T, W, Rd, vx.p, 0);
+            k_check<<<g, 128, 0, s>>>(T, W, Rd, 0);
+            k_restar<<<g, 128, 0, s>>>(T, W, Rd, 0);
+            int hc[3] = {0, 0, 0};
+            uint32_t hs = 0;
+            D3G_CUDA(cudaMemcpyAsync(hc, counters.p, sizeof hc, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaStreamSynchronize(s));
+            if (hs != 0) {
+                const int st = status_from_bits(hs);
+                if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");
+                return st;
+            }
+            if (hc[1] > 0) {
+                set_error("d3g_build: a conflict region exceeded the per-worker scratch");
+                return D3G_ERR_CAVITY_CAPACITY;
+            }
+            won += hc[2];
+            attempts += hc[0] + hc[2];
+            if (hc[0] == 0) break;
+            if (hc[2] == 0) {   // the earliest pending point must always win
+                set_error("d3g_build: an insertion round made no progress");
+                return D3G_ERR_INTERNAL;
+            }
+        }
+        if (trace) {
+            cudaEventRecord(ev1, s);
+            cudaEventSynchronize(ev1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            fprintf(stderr, "d3g level [%d,%d) workers %d rounds %d inserted %lld attempts %lld ms %.2f\n",
+                    lb, le, W.n, round - round0, won, attempts, ms);
+            cudaEventDestroy(ev0);
+            cudaEventDestroy(ev1);
+        }
+    }
+    R.rounds = round;
+    // Release round scratch before the output stage.
+    wcav.release();
+    wfac.release();
+    wsv.release();
+    wsn.release();
+    claim.release();
+    fnew.release();
+
+    // ---- output: canonical cells ----
+    int ntet = 0;
+    D3G_CUDA(cudaMemcpyAsync(&ntet, tet_count.p, sizeof ntet, cudaMemcpyDeviceToHost, s));
+    D3G_CUDA(cudaStreamSynchronize(s));
+    const int kbits = bits_for(uint64_t(N) + 1);
+    for (int pass = 0; pass < (opt.want_all_cells ? 2 : 1); ++pass) {
+        const bool with_inf = pass == 1;
+        DevBuf<int32_t> flag, pos, idx;
+        D3G_TRY(flag.alloc(size_t(ntet), s));
+        D3G_TRY(pos.alloc(size_t(ntet), s));
+        k_cell_flags<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, alive.p, ntet, with_inf, flag.p);
+        D3G_TRY(exclusive_scan(flag.p, pos.p, ntet, s));
+        int last_pos = 0, last_flag = 0;
+        D3G_CUDA(cudaMemcpyAsync(&last_pos, pos.p + ntet - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaMemcpyAsync(&last_flag, flag.p + ntet - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));
+        const int64_t nc = int64_t(last_pos) + last_flag;
+        DevBuf<int4> raw;
+        DevBuf<unsigned long long> khi, klo;
+        D3G_TRY(raw.alloc(size_t(nc), s));
+        D3G_TRY(khi.alloc(size_t(nc), s));
+        D3G_TRY(klo.alloc(size_t(nc), s));
+        D3G_TRY(idx.alloc(size_t(nc), s));
+        k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, kbits,
+                                                        raw.p, khi.p, klo.p, idx.p);
+        if (!with_inf) {
+            D3G_TRY(sort_cells(raw, khi, klo, idx, nc, kbits, R.cells, s));
+            R.n_cells = nc;
+        } else {
+            D3G_TRY(sort_cells(raw, khi, klo, idx, nc, kbits, R.all, s));
+            R.n_all = nc;
+        }
+    }
+    if (opt.want_incident) {
+        const int64_t m = 4 * R.n_cells;
+        DevBuf<int32_t> pt, cell, pt2, cnt;
+        D3G_TRY(R.inc_off.alloc(size_t(N) + 1, s));
+        D3G_TRY(R.inc.alloc(size_t(m > 0 ? m : 1), s));
+        D3G_TRY(cnt.alloc(size_t(N) + 1, s));
+        D3G_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * (size_t(N) + 1), s));
+        if (m > 0) {
+            D3G_TRY(pt.alloc(size_t(m), s));
+            D3G_TRY(cell.alloc(size_t(m), s));
+            D3G_TRY(pt2.alloc(size_t(m), s));
+            k_incident_pairs<<<grid_for(R.n_cells, 256), 256, 0, s>>>(R.cells.p, R.n_cells, pt.p, cell.p,
+                                                                     cnt.p);
+            D3G_TRY(sort_pairs(pt.p, pt2.p, cell.p, R.inc.p, m, 0, bits_for(uint64_t(N)), s));
+        }
+        DevBuf<int64_t> cnt64;
+        D3G_TRY(cnt64.alloc(size_t(N) + 1, s));
+        k_widen<<<grid_for(n + 1, 256), 256, 0, s>>>(cnt.p, n + 1, cnt64.p);
+        D3G_TRY(exclusive_scan(cnt64.p, R.inc_off.p, n + 1, s));
+        R.n_inc = m;
+    }
+    D3G_CUDA(cudaGetLastError());
+    D3G_CUDA(cudaMemcpyAsync(hst, status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    D3G_CUDA(cudaStreamSynchronize(s));
+    return status_from_bits(hst[0]);
+}
+
+}  // namespace d3g
+
+using namespace d3g;
+
+extern "C" {
+
+void d3g_options_default(d3g_options* o) {
+    if (!o) return;
+    o->want_all_cells = 1;
+    o->want_incident = 1;
+    o->chunk = 0;
+    o->max_rounds = 0;
+}
+
+void d3g_result_free(d3g_result* r) {
+    if (!r) return;
+    free(r->cells);
+    free(r->all_cells);
+    free(r->incident_offsets);
+    free(r->incident);
+    *r = d3g_result{};
+}
+
+int d3g_build(const double* xyz, int64_t n, const d3g_options* opts, d3g_result* out) {
+    if (!out || n < 0 || (n > 0 && !xyz)) return D3G_ERR_INVALID_ARGUMENT;
+    *out = d3g_result{};
+    d3g_options o;
+    d3g_options_default(&o);
+    if (opts) o = *opts;
+    out->n_points = n;
+    if (n == 0) {
+        out->incident_offsets = static_cast<int64_t*>(calloc(1, sizeof(int64_t)));
+        return D3G_OK;
+    }
+    D3G_TRY(ensure_device());
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st;
+    DeviceResult R;
+    {
+        DevBuf<double> dx;
+        D3G_TRY(dx.alloc(size_t(3 * n), s));
+        D3G_CUDA(cudaMemcpyAsync(dx.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+        cudaEventRecord(e0, s);
+        st = build_device_impl(dx.p, n, o, s, R);
+        cudaEventRecord(e1, s);
+    }
+    if (st == D3G_OK) {
+        out->n_vertices = R.n_vertices;
+        out->n_cells = R.n_cells;
+        out->n_all = R.n_all;
+        out->rounds = R.rounds;
+        out->cells = static_cast<int32_t*>(malloc(sizeof(int32_t) * 4 * size_t(R.n_cells > 0 ? R.n_cells : 1)));
+        if (R.n_cells > 0)
+            cudaMemcpyAsync(out->cells, R.cells.p, sizeof(int4) * R.n_cells, cudaMemcpyDeviceToHost, s);
+        if (o.want_all_cells) {
+            out->all_cells = static_cast<int32_t*>(malloc(sizeof(int32_t) * 4 * size_t(R.n_all > 0 ? R.n_all : 1)));
+            if (R.n_all > 0)
+                cudaMemcpyAsync(out->all_cells, R.all.p, sizeof(int4) * R.n_all, cudaMemcpyDeviceToHost, s);
+        }
+        if (o.want_incident) {
+            out->incident_offsets = static_cast<int64_t*>(malloc(sizeof(int64_t) * (size_t(n) + 1)));
+            out->incident = static_cast<int32_t*>(malloc(sizeof(int32_t) * size_t(R.n_inc > 0 ? R.n_inc : 1)));
+            cudaMemcpyAsync(out->incident_offsets, R.inc_off.p, sizeof(int64_t) * (n + 1),
+                            cudaMemcpyDeviceToHost, s);
+            if (R.n_inc > 0)
+                cudaMemcpyAsync(out->incident, R.inc.p, sizeof(int32_t) * R.n_inc, cudaMemcpyDeviceToHost, s);
+        }
+        const cudaError_t e = cudaStreamSynchronize(s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        out->device_ms = ms;
+        if (e != cudaSuccess) {
+            set_error(std::string("d3g_build: ") + cudaGetErrorString(e));
+            st = D3G_ERR_CUDA;
+        }
+    }
+    R.reset();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != D3G_OK) d3g_result_free(out);
+    return st;
+}
+
+int d3g_build_device(const double* d_xyz, int64_t n, const d3g_options* opts, int32_t* d_cells,
+                     int64_t cap_cells, int64_t* n_cells_out, int64_t* n_vertices_out, void* stream) {
+    if (n < 0 || (n > 0 && !d_xyz) || cap_cells < 0) return D3G_ERR_INVALID_ARGUMENT;
+    d3g_options o;
+    d3g_options_default(&o);
+    if (opts) o = *opts;
+    o.want_all_cells = 0;
+    o.want_incident = 0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DeviceResult R;
+    const int st = build_device_impl(d_xyz, n, o, s, R);
+    if (st != D3G_OK) return st;
+    if (n_cells_out) *n_cells_out = R.n_cells;
+    if (n_vertices_out) *n_vertices_out = R.n_vertices;
+    if (R.n_cells > cap_cells) {
+        set_error("d3g_build_device: output capacity too small");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    if (R.n_cells > 0) {
+        if (!d_cells) return D3G_ERR_INVALID_ARGUMENT;
+        D3G_CUDA(cudaMemcpyAsync(d_cells, R.cells.p, sizeof(int4) * R.n_cells, cudaMemcpyDeviceToDevice, s));
+    }
+    R.reset();
+    D3G_CUDA(cudaStreamSynchronize(s));
+    return D3G_OK;
+}
+
+}  // extern "C"

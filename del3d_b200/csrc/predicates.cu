@@ -1,0 +1,253 @@
+// Batch predicate evaluation: the C ABI d3g_predicates / d3g_predicates_device.
+//
+// orient3d and in_sphere run in two kernels:
+//   k_filter_*  one thread per query: gather the points, evaluate the filter;
+//               certain queries write their sign, uncertain ones are appended
+//               to a compacted queue with one warp-aggregated atomic per warp;
+//   k_exact_*   one thread per queued query: the exact stage and, for
+//               in_sphere, the symbolic perturbation.
+// The filter kernel is bound by the point gathers (HBM/L2) and the FP64 pipe;
+// the queue keeps the rare, long-running exact path out of its warps.
+// The coplanar family, used only on hull-coplanar configurations, runs as one
+// kernel per query.
+#include "common.cuh"
+
+namespace d3g {
+namespace {
+
+__device__ __forceinline__ Pt load_pt(const double* __restrict__ pts, int32_t i) {
+    const double* p = pts + 3 * int64_t(i);
+    return Pt{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+}
+
+__device__ __forceinline__ bool idx_ok(int32_t i, int64_t n) { return i >= 0 && int64_t(i) < n; }
+
+/// Appends `q` to the queue if `push`; all lanes of the warp must call this.
+__device__ __forceinline__ void warp_push(bool push, int64_t q, int64_t* queue,
+                                          unsigned long long* count) {
+    const unsigned mask = __ballot_sync(0xffffffffu, push);
+    if (mask == 0) return;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == __ffs(mask) - 1) base = atomicAdd(count, (unsigned long long)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+    if (push) queue[base + __popc(mask & ((1u << lane) - 1u))] = q;
+}
+
+__global__ void __launch_bounds__(256) k_filter_orient3d(const double* __restrict__ pts, int64_t npts,
+                                                         const int32_t* __restrict__ idx, int64_t nq,
+                                                         int8_t* __restrict__ out, int64_t* queue,
+                                                         unsigned long long* qcount, uint32_t* status) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t nq_pad = (nq + 31) & ~int64_t(31);
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq_pad; q += stride) {
+        bool push = false;
+        if (q < nq) {
+            const int4 t = *reinterpret_cast<const int4*>(idx + 4 * q);
+            if (idx_ok(t.x, npts) && idx_ok(t.y, npts) && idx_ok(t.z, npts) && idx_ok(t.w, npts)) {
+                const Orient3dFilter f = orient3d_filter(load_pt(pts, t.x), load_pt(pts, t.y),
+                                                         load_pt(pts, t.z), load_pt(pts, t.w));
+                out[q] = int8_t(f.certain ? -sign_of(f.det) : 0);
+                push = !f.certain;
+            } else {
+                out[q] = 0;
+                report(status, ST_INTERNAL);
+            }
+        }
+        warp_push(push, q, queue, qcount);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_exact_orient3d(const double* __restrict__ pts,
+                                                        const int32_t* __restrict__ idx,
+                                                        int8_t* __restrict__ out,
+                                                        const int64_t* __restrict__ queue,
+                                                        const unsigned long long* qcount,
+                                                        uint32_t* status) {
+    const int64_t n = int64_t(*qcount);
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t q = queue[k];
+        const int4 t = *reinterpret_cast<const int4*>(idx + 4 * q);
+        const Pt a = load_pt(pts, t.x), b = load_pt(pts, t.y), c = load_pt(pts, t.z),
+                 d = load_pt(pts, t.w);
+        const Orient3dFilter f = orient3d_filter(a, b, c, d);
+        out[q] = int8_t(orient3d_exact(a, b, c, d, f.det, status));
+    }
+}
+
+__global__ void __launch_bounds__(256) k_filter_in_sphere(const double* __restrict__ pts, int64_t npts,
+                                                          const int32_t* __restrict__ idx, int64_t nq,
+                                                          int8_t* __restrict__ out, int64_t* queue,
+                                                          unsigned long long* qcount, uint32_t* status) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t nq_pad = (nq + 31) & ~int64_t(31);
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq_pad; q += stride) {
+        bool push = false;
+        if (q < nq) {
+            const int32_t* t = idx + 5 * q;
+            const int32_t i0 = t[0], i1 = t[1], i2 = t[2], i3 = t[3], i4 = t[4];
+            if (idx_ok(i0, npts) && idx_ok(i1, npts) && idx_ok(i2, npts) && idx_ok(i3, npts) &&
+                idx_ok(i4, npts)) {
+                const InSphereFilter f =
+                    in_sphere_filter(load_pt(pts, i0), load_pt(pts, i1), load_pt(pts, i2),
+                                     load_pt(pts, i3), load_pt(pts, i4));
+                out[q] = int8_t(f.certain ? -sign_of(f.det) : 0);
+                push = !f.certain;
+            } else {
+                out[q] = 0;
+                report(status, ST_INTERNAL);
+            }
+        }
+        warp_push(push, q, queue, qcount);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_exact_in_sphere(const double* __restrict__ pts,
+                                                         const int32_t* __restrict__ idx,
+                                                         int8_t* __restrict__ out,
+                                                         const int64_t* __restrict__ queue,
+                                                         const unsigned long long* qcount,
+                                                         int perturbed, uint32_t* status) {
+    const int64_t n = int64_t(*qcount);
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t q = queue[k];
+        const int32_t* t = idx + 5 * q;
+        const int64_t id[5] = {t[0], t[1], t[2], t[3], t[4]};
+        const Pt a = load_pt(pts, t[0]), b = load_pt(pts, t[1]), c = load_pt(pts, t[2]),
+                 d = load_pt(pts, t[3]), e = load_pt(pts, t[4]);
+        const InSphereFilter f = in_sphere_filter(a, b, c, d, e);
+        int s = in_sphere_exact(a, b, c, d, e, f.det, status);
+        if (s == 0 && perturbed) s = in_sphere_perturb(a, b, c, d, e, id, status);
+        out[q] = int8_t(s);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_coplanar(const double* __restrict__ pts, int64_t npts,
+                                                  const int32_t* __restrict__ idx, int64_t nq,
+                                                  int kind, int8_t* __restrict__ out,
+                                                  unsigned long long* nexact, uint32_t* status) {
+    const int k = (kind == D3G_COPLANAR_ORIENTATION3 || kind == D3G_COLLINEAR) ? 3 : 4;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq;
+         q += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t* t = idx + k * q;
+        bool ok = true;
+        for (int j = 0; j < k; ++j) ok = ok && idx_ok(t[j], npts);
+        if (!ok) {
+            out[q] = 0;
+            report(status, ST_INTERNAL);
+            continue;
+        }
+        const Pt p0 = load_pt(pts, t[0]), p1 = load_pt(pts, t[1]), p2 = load_pt(pts, t[2]);
+        int s = 0;
+        switch (kind) {
+            case D3G_COPLANAR_ORIENTATION3: s = coplanar_orientation3(p0, p1, p2, status); break;
+            case D3G_COLLINEAR: s = collinear(p0, p1, p2, status) ? 1 : 0; break;
+            case D3G_COPLANAR_ORIENTATION4:
+                s = coplanar_orientation4(p0, p1, p2, load_pt(pts, t[3]), status);
+                break;
+            default: {
+                const Pt p3 = load_pt(pts, t[3]);
+                const InCircleFilter f = in_circle_filter(p0, p1, p2, p3);
+                if (f.certain) {
+                    s = sign_of(f.det);
+                } else {
+                    atomicAdd(nexact, 1ull);
+                    s = in_circle_exact(p0, p1, p2, p3, f.det, status);
+                    if (s == 0 && kind == D3G_COPLANAR_IN_CIRCLE) {
+                        const int64_t id[4] = {t[0], t[1], t[2], t[3]};
+                        s = in_circle_perturb(p0, p1, p2, p3, id, status);
+                    }
+                }
+            }
+        }
+        out[q] = int8_t(s);
+    }
+}
+
+__global__ void k_orient2d(const double* __restrict__ six, int64_t nq, int8_t* __restrict__ out,
+                           uint32_t* status) {
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq;
+         q += int64_t(gridDim.x) * blockDim.x) {
+        const double* s = six + 6 * q;
+        out[q] = int8_t(orient2d(s[0], s[1], s[2], s[3], s[4], s[5], status));
+    }
+}
+
+}  // namespace
+
+int predicates_device(const double* d_pts, int64_t n_pts, const int32_t* d_idx, int64_t nq, int kind,
+                      int8_t* d_out, cudaStream_t stream, d3g_predicate_stats* stats) {
+    if (nq < 0 || n_pts < 0 || d3g_predicate_arity(kind) == 0) {
+        set_error("d3g_predicates: bad size or kind");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    if (nq == 0) {
+        if (stats) *stats = d3g_predicate_stats{0, 0};
+        return D3G_OK;
+    }
+    if (!d_pts || !d_idx || !d_out) {
+        set_error("d3g_predicates: null pointer");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    if (kind == D3G_ORIENT3D && (reinterpret_cast<uintptr_t>(d_idx) & 15u) != 0) {
+        set_error("d3g_predicates: orient3d index array must be 16-byte aligned");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    // Scratch: status word, queue counter, and the exact-stage queue.
+    DevBuf<unsigned long long> counters;
+    D3G_TRY(counters.alloc(2, stream));
+    D3G_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(unsigned long long), stream));
+    uint32_t* status = reinterpret_cast<uint32_t*>(counters.p);
+    unsigned long long* qcount = counters.p + 1;
+    DevBuf<int64_t> queue;
+    const int blk = 256;
+    if (kind == D3G_ORIENT3D || kind == D3G_IN_SPHERE || kind == D3G_IN_SPHERE_UNPERTURBED) {
+        D3G_TRY(queue.alloc(size_t(nq), stream));
+        const unsigned g = grid_for(nq, blk, int64_t(kNumSMs) * 16);
+        if (kind == D3G_ORIENT3D) {
+            k_filter_orient3d<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, queue.p, qcount,
+                                                     status);
+            k_exact_orient3d<<<kNumSMs * 4, 256, 0, stream>>>(d_pts, d_idx, d_out, queue.p, qcount,
+                                                             status);
+        } else {
+            k_filter_in_sphere<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, queue.p,
+                                                      qcount, status);
+            k_exact_in_sphere<<<kNumSMs * 8, 128, 0, stream>>>(
+                d_pts, d_idx, d_out, queue.p, qcount, kind == D3G_IN_SPHERE ? 1 : 0, status);
+        }
+    } else {
+        k_coplanar<<<grid_for(nq, 128), 128, 0, stream>>>(d_pts, n_pts, d_idx, nq, kind, d_out,
+                                                          qcount, status);
+    }
+    D3G_CUDA(cudaGetLastError());
+    unsigned long long host_counters[2] = {0, 0};
+    D3G_CUDA(cudaMemcpyAsync(host_counters, counters.p, sizeof host_counters, cudaMemcpyDeviceToHost,
+                             stream));
+    queue.release();
+    counters.release();
+    D3G_CUDA(cudaStreamSynchronize(stream));
+    if (stats) *stats = d3g_predicate_stats{nq, int64_t(host_counters[1])};
+    const uint32_t bits = uint32_t(host_counters[0]);
+    if (bits & ST_INTERNAL) {
+        set_error("d3g_predicates: point index out of range");
+        return D3G_ERR_INVALID_INPUT;
+    }
+    return status_from_bits(bits);
+}
+
+int orient2d_device(const double* d_six, int64_t nq, int8_t* d_out, cudaStream_t stream) {
+    DevBuf<uint32_t> st;
+    D3G_TRY(st.alloc(1, stream));
+    D3G_CUDA(cudaMemsetAsync(st.p, 0, sizeof(uint32_t), stream));
+    if (nq > 0) k_orient2d<<<grid_for(nq, 128), 128, 0, stream>>>(d_six, nq, d_out, st.p);
+    D3G_CUDA(cudaGetLastError());
+    uint32_t bits = 0;
+    D3G_CUDA(cudaMemcpyAsync(&bits, st.p, sizeof bits, cudaMemcpyDeviceToHost, stream));
+    st.release();
+    D3G_CUDA(cudaStreamSynchronize(stream));
+    return status_from_bits(bits);
+}
+
+}  // namespace d3g

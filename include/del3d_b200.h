@@ -1,0 +1,151 @@
+/*
+ * del3d_b200 - C ABI of the B200 (sm_100a) implementation of del3d's
+ * Delaunay::build hot path.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a d3g_status; none
+ * aborts.  Entry points whose name ends in _device take device pointers and a
+ * cudaStream_t (passed as void*; NULL = the legacy default stream) and run
+ * asynchronously on that stream unless stated otherwise; the others take host
+ * pointers, copy in and out, and return when the result is on the host.
+ *
+ * Reference interfaces replaced (paths inside the del3d source tree):
+ *   del3d::orient3d / in_sphere / in_sphere_unperturbed  include/del3d/predicates.h:28,52,57
+ *   del3d::orient2d / coplanar_orientation (x2) / collinear /
+ *     coplanar_in_circle(_unperturbed)                    include/del3d/predicates2.h:27-70
+ *   del3d::spatial_sort                                    include/del3d/spatial_sort.h:37
+ *   del3d::Delaunay::build / finite_cells / all_cells /
+ *     incident_cells / number_of_vertices                  include/del3d/delaunay.h:68-85
+ *
+ * Documented difference from the reference: finite_cells() comes back in a
+ * canonical order instead of the reference's cell-allocation order.  Each tet
+ * is rotated by an even permutation (orientation preserved) so that its
+ * smallest point index comes first and the other three follow in the cyclic
+ * order that starts with their smallest; tets are then sorted
+ * lexicographically.  The SET of tets is identical to the reference's.
+ */
+#ifndef DEL3D_B200_H
+#define DEL3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum d3g_status {
+    D3G_OK = 0,
+    D3G_ERR_INVALID_ARGUMENT = 1, /* null pointer, negative size, unknown kind   */
+    D3G_ERR_INVALID_INPUT = 2,    /* non-finite coordinate or out-of-range index */
+    D3G_ERR_OOM = 3,              /* a device allocation failed                  */
+    D3G_ERR_EXACT_CAPACITY = 4,   /* exponent span too wide for the exact stage  */
+    D3G_ERR_CAVITY_CAPACITY = 5,  /* a conflict region outgrew its scratch space */
+    D3G_ERR_WALK_LIMIT = 6,       /* a point-location walk hit its step limit    */
+    D3G_ERR_ROUND_LIMIT = 7,      /* insertion rounds hit their limit            */
+    D3G_ERR_CUDA = 8,             /* a CUDA runtime call failed                  */
+    D3G_ERR_INTERNAL = 9,         /* an internal invariant did not hold          */
+    D3G_ERR_NO_DEVICE = 10        /* no CUDA device could be used                */
+} d3g_status;
+
+/* Human-readable name of a status; never NULL. */
+const char* d3g_status_string(int status);
+/* Detail of the last error on the calling thread ("" if none). */
+const char* d3g_last_error(void);
+
+/* ---- predicates ------------------------------------------------------------
+ * Batch evaluation over index tuples into a point table `pts` (3 doubles per
+ * point, x y z).  `idx` holds k int32 indices per query, k given by the kind;
+ * `sign_out` receives one int8 per query: -1, 0, +1 (collinear: 1 true, 0 false).
+ * Signs equal the reference functions named below on the same points, with
+ * "the same point" meaning the same index (the reference compares pointers).
+ */
+typedef enum d3g_predicate {
+    D3G_ORIENT3D = 0,                      /* k=4  del3d::orient3d(a,b,c,d)                */
+    D3G_IN_SPHERE = 1,                     /* k=5  del3d::in_sphere(a,b,c,d,e)             */
+    D3G_IN_SPHERE_UNPERTURBED = 2,         /* k=5  del3d::in_sphere_unperturbed            */
+    D3G_COPLANAR_ORIENTATION3 = 3,         /* k=3  del3d::coplanar_orientation(p,q,r)      */
+    D3G_COPLANAR_ORIENTATION4 = 4,         /* k=4  del3d::coplanar_orientation(p,q,r,s)    */
+    D3G_COPLANAR_IN_CIRCLE = 5,            /* k=4  del3d::coplanar_in_circle(p0,p1,p2,p)   */
+    D3G_COPLANAR_IN_CIRCLE_UNPERTURBED = 6,/* k=4  del3d::coplanar_in_circle_unperturbed   */
+    D3G_COLLINEAR = 7                      /* k=3  del3d::collinear(p,q,r)                 */
+} d3g_predicate;
+
+/* Queries per kind (k above); 0 for an unknown kind. */
+int d3g_predicate_arity(int kind);
+
+typedef struct d3g_predicate_stats {
+    int64_t n_queries;     /* queries evaluated                              */
+    int64_t n_exact;       /* of which the filter left uncertain (exact stage) */
+} d3g_predicate_stats;
+
+/* Host pointers; synchronous.  `stats` may be NULL. */
+int d3g_predicates(const double* pts, int64_t n_pts, const int32_t* idx, int64_t n_queries,
+                   int kind, int8_t* sign_out, d3g_predicate_stats* stats);
+
+/* Device pointers on `stream`.  Reads the status back, so it synchronises
+ * `stream` before returning.  `stats` (host pointer) may be NULL. */
+int d3g_predicates_device(const double* d_pts, int64_t n_pts, const int32_t* d_idx,
+                          int64_t n_queries, int kind, int8_t* d_sign_out, void* stream,
+                          d3g_predicate_stats* stats);
+
+/* del3d::orient2d(px,py,qx,qy,rx,ry) over `six` (6 doubles per query); host pointers. */
+int d3g_orient2d(const double* six, int64_t n_queries, int8_t* sign_out);
+
+/* ---- spatial sort ----------------------------------------------------------
+ * The reference insertion order (rand48 shuffle, multiscale split, Hilbert
+ * median splits), bit for bit: order[k] = index of the k-th point. */
+int d3g_spatial_sort(const double* xyz, int64_t n, int32_t* order);
+int d3g_spatial_sort_device(const double* d_xyz, int64_t n, int32_t* d_order, void* stream);
+
+/* ---- the build ---------------------------------------------------------------
+ * A d3g_result holds one triangulation on the host.  It owns its arrays; free
+ * it with d3g_result_free.  Fields are valid until then. */
+typedef struct d3g_result {
+    int64_t n_points;        /* input size                                       */
+    int64_t n_vertices;      /* distinct points (number_of_vertices())           */
+    int64_t n_cells;         /* finite tets                                      */
+    int32_t* cells;          /* n_cells x 4, canonical order (finite_cells())    */
+    int64_t n_all;           /* all tets, infinite ones included                 */
+    int32_t* all_cells;      /* n_all x 4, -1 = the infinite vertex, canonical   */
+    int64_t* incident_offsets; /* n_points + 1 (CSR of incident_cells())         */
+    int32_t* incident;       /* incident_offsets[n_points] finite-cell indices   */
+    /* build statistics */
+    int32_t rounds;          /* insertion rounds                                 */
+    int64_t n_exact;         /* predicate calls that reached the exact stage     */
+    double device_ms;        /* device time of the build (CUDA events)           */
+} d3g_result;
+
+typedef struct d3g_options {
+    int32_t want_all_cells;  /* also produce all_cells                           */
+    int32_t want_incident;   /* also produce incident_cells                      */
+    int32_t chunk;           /* points per worker chunk (0 = default)            */
+    int32_t max_rounds;      /* 0 = default                                      */
+} d3g_options;
+
+/* Fills `opts` with the defaults (all outputs on). */
+void d3g_options_default(d3g_options* opts);
+
+/* del3d::Delaunay::build over host points (3 doubles per point).  `opts` may be
+ * NULL.  On success *out owns the result (free with d3g_result_free); on error
+ * *out is left zeroed. */
+int d3g_build(const double* xyz, int64_t n, const d3g_options* opts, d3g_result* out);
+void d3g_result_free(d3g_result* r);
+
+/* The same build over device-resident points, writing the canonical finite
+ * cells into a caller-supplied device array of `cap_cells` x 4 int32 on
+ * `stream`.  *n_cells_out receives the cell count (also when it exceeds
+ * cap_cells, in which case nothing is written and D3G_ERR_INVALID_ARGUMENT is
+ * returned).  Synchronises `stream`. */
+int d3g_build_device(const double* d_xyz, int64_t n, const d3g_options* opts, int32_t* d_cells,
+                     int64_t cap_cells, int64_t* n_cells_out, int64_t* n_vertices_out,
+                     void* stream);
+
+/* ---- synthetic inputs (host) -------------------------------------------------
+ * Deterministic generators (std::mt19937 with u01 = word * 2^-32, written out). */
+void d3g_gen_uniform(int64_t n, uint32_t seed, double lo, double hi, double* xyz);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEL3D_B200_H */

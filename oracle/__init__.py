@@ -1,0 +1,290 @@
+"""Parity checkers for the del3d ``Delaunay::build`` path.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import this
+package, and only as the checker or the timed CPU baseline -- never as part of
+the product path (``del3d_b200`` never imports it).
+
+Two libraries are loaded through ctypes:
+
+* ``liboracle.so`` -- our CPU restatement of the reference algorithm
+  (``oracle/oracle.cpp``: predicates, rand48 + Hilbert spatial sort, sequential
+  Bowyer-Watson build, canonical cell order);
+* ``_ref/libdel3d_ref.so`` -- the reference del3d compiled from its own sources
+  (``oracle/Makefile``) plus its integer oracle ``tests/exact.h`` and its test
+  point-set generators ``tests/pointsets.h``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ORC_PATH = os.path.join(_HERE, "liboracle.so")
+_REF_PATH = os.path.join(_HERE, "_ref", "libdel3d_ref.so")
+
+_orc: Optional[ctypes.CDLL] = None
+_ref: Optional[ctypes.CDLL] = None
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_INT = ctypes.c_int
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def orc() -> ctypes.CDLL:
+    global _orc
+    if _orc is None:
+        lib = ctypes.CDLL(_ORC_PATH)
+        for name in ("orc_orient3d", "orc_coplanar_orientation3", "orc_coplanar_orientation4",
+                     "orc_collinear"):
+            getattr(lib, name).argtypes = [_P, _P, _I64, _P]
+        for name in ("orc_in_sphere", "orc_coplanar_in_circle"):
+            getattr(lib, name).argtypes = [_P, _P, _I64, _INT, _P]
+        lib.orc_orient2d.argtypes = [_P, _I64, _P]
+        lib.orc_spatial_sort.argtypes = [_P, _I64, _P]
+        lib.orc_shuffle.argtypes = [_I64, _P]
+        lib.orc_build.argtypes = [_P, _I64]
+        lib.orc_build.restype = _P
+        for name in ("orc_build_ncells", "orc_build_nall", "orc_build_nvertices"):
+            getattr(lib, name).argtypes = [_P]
+            getattr(lib, name).restype = _I64
+        lib.orc_build_cells.argtypes = [_P, _P]
+        lib.orc_build_all.argtypes = [_P, _P]
+        lib.orc_build_free.argtypes = [_P]
+        lib.orc_canonical_rotate.argtypes = [_P, _I64]
+        _orc = lib
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF_PATH)
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        lib = ctypes.CDLL(_REF_PATH)
+        for name in ("ref_orient3d", "ref_coplanar_orientation3", "ref_coplanar_orientation4",
+                     "ref_collinear", "exact_orient3d", "exact_coplanar_orientation3",
+                     "exact_coplanar_orientation4", "exact_collinear"):
+            getattr(lib, name).argtypes = [_P, _P, _I64, _P]
+        for name in ("ref_in_sphere", "ref_coplanar_in_circle", "exact_in_sphere",
+                     "exact_coplanar_in_circle"):
+            getattr(lib, name).argtypes = [_P, _P, _I64, _INT, _P]
+        lib.ref_orient2d.argtypes = [_P, _I64, _P]
+        lib.ref_spatial_sort.argtypes = [_P, _I64, _P]
+        lib.ref_build.argtypes = [_P, _I64]
+        lib.ref_build.restype = _P
+        for name in ("ref_build_ncells", "ref_build_nall", "ref_build_nvertices"):
+            getattr(lib, name).argtypes = [_P]
+            getattr(lib, name).restype = _I64
+        lib.ref_build_cells.argtypes = [_P, _P]
+        lib.ref_build_all.argtypes = [_P, _P]
+        lib.ref_build_incident.argtypes = [_P, _P, _P]
+        lib.ref_build_incident.restype = _I64
+        lib.ref_build_free.argtypes = [_P]
+        lib.ref_build_time.argtypes = [_P, _I64, _P]
+        lib.ref_build_time.restype = ctypes.c_double
+        lib.ref_circumcenter.argtypes = [_P, _P, _I64, _INT, _P]
+        for name, args in (("ps_cylinder", [_I64, _INT, ctypes.c_uint, _P]),
+                           ("ps_sphere", [_I64, _INT, ctypes.c_uint, _P]),
+                           ("ps_torus", [_I64, _INT, ctypes.c_uint, _P]),
+                           ("ps_box_shell", [_INT, _P]),
+                           ("ps_lattice", [_INT, _INT, _INT, _P]),
+                           ("ps_random_cube", [_I64, ctypes.c_uint, _P])):
+            getattr(lib, name).argtypes = args
+            getattr(lib, name).restype = _I64
+        lib.ps_rng_below.argtypes = [ctypes.c_uint, _I64, _I64, _P]
+        _ref = lib
+    return _ref
+
+
+# ---- helpers -------------------------------------------------------------------
+
+_ARITY = {"orient3d": 4, "in_sphere": 5, "in_sphere_unperturbed": 5, "coplanar_orientation3": 3,
+          "coplanar_orientation4": 4, "coplanar_in_circle": 4,
+          "coplanar_in_circle_unperturbed": 4, "collinear": 3}
+
+
+def _pred(lib: ctypes.CDLL, prefix: str, kind: str, pts: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    k = _ARITY[kind]
+    assert idx.ndim == 2 and idx.shape[1] == k
+    out = np.zeros(idx.shape[0], dtype=np.int8)
+    nq = idx.shape[0]
+    if kind in ("in_sphere", "in_sphere_unperturbed"):
+        getattr(lib, prefix + "in_sphere")(_ptr(pts), _ptr(idx), nq, int(kind == "in_sphere"), _ptr(out))
+    elif kind in ("coplanar_in_circle", "coplanar_in_circle_unperturbed"):
+        getattr(lib, prefix + "coplanar_in_circle")(_ptr(pts), _ptr(idx), nq,
+                                                    int(kind == "coplanar_in_circle"), _ptr(out))
+    else:
+        getattr(lib, prefix + kind)(_ptr(pts), _ptr(idx), nq, _ptr(out))
+    return out
+
+
+def orc_predicate(kind: str, pts: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    return _pred(orc(), "orc_", kind, pts, idx)
+
+
+def ref_predicate(kind: str, pts: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    return _pred(ref(), "ref_", kind, pts, idx)
+
+
+def exact_predicate(kind: str, pts: np.ndarray, idx: np.ndarray) -> np.ndarray:
+    return _pred(ref(), "exact_", kind, pts, idx)
+
+
+def orc_spatial_sort(pts: np.ndarray) -> np.ndarray:
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    out = np.zeros(pts.shape[0], dtype=np.int32)
+    orc().orc_spatial_sort(_ptr(pts), pts.shape[0], _ptr(out))
+    return out
+
+
+def orc_shuffle(n: int) -> np.ndarray:
+    out = np.zeros(n, dtype=np.int32)
+    orc().orc_shuffle(n, _ptr(out))
+    return out
+
+
+def ref_spatial_sort(pts: np.ndarray) -> np.ndarray:
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    out = np.zeros(pts.shape[0], dtype=np.int32)
+    ref().ref_spatial_sort(_ptr(pts), pts.shape[0], _ptr(out))
+    return out
+
+
+def orc_build(pts: np.ndarray) -> dict:
+    """Canonical cells (and all cells) of our CPU restatement."""
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    lib = orc()
+    h = lib.orc_build(_ptr(pts), pts.shape[0])
+    if not h:
+        raise ValueError("non-finite input")
+    try:
+        nc, na = lib.orc_build_ncells(h), lib.orc_build_nall(h)
+        cells = np.zeros((nc, 4), dtype=np.int32)
+        allc = np.zeros((na, 4), dtype=np.int32)
+        if nc:
+            lib.orc_build_cells(h, _ptr(cells))
+        if na:
+            lib.orc_build_all(h, _ptr(allc))
+        return {"cells": cells, "all": allc, "n_vertices": lib.orc_build_nvertices(h)}
+    finally:
+        lib.orc_build_free(h)
+
+
+def ref_build(pts: np.ndarray) -> dict:
+    """The reference build's outputs, in the reference's own (allocation) order."""
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    lib = ref()
+    h = lib.ref_build(_ptr(pts), pts.shape[0])
+    try:
+        nc, na = lib.ref_build_ncells(h), lib.ref_build_nall(h)
+        cells = np.zeros((nc, 4), dtype=np.int32)
+        allc = np.zeros((na, 4), dtype=np.int32)
+        if nc:
+            lib.ref_build_cells(h, _ptr(cells))
+        if na:
+            lib.ref_build_all(h, _ptr(allc))
+        ninc = lib.ref_build_incident(h, None, None)
+        offs = np.zeros(pts.shape[0] + 1, dtype=np.int64)
+        data = np.zeros(max(ninc, 1), dtype=np.int32)
+        lib.ref_build_incident(h, _ptr(offs), _ptr(data))
+        return {"cells": cells, "all": allc, "n_vertices": lib.ref_build_nvertices(h),
+                "incident_offsets": offs, "incident": data[:ninc]}
+    finally:
+        lib.ref_build_free(h)
+
+
+def canonical_rotate(tets: np.ndarray) -> np.ndarray:
+    t = np.ascontiguousarray(tets, dtype=np.int32).copy()
+    if t.shape[0]:
+        orc().orc_canonical_rotate(_ptr(t), t.shape[0])
+    return t
+
+
+def canonical_cells(tets: np.ndarray) -> np.ndarray:
+    """Even rotation per tet, then lexicographic sort of the tets."""
+    t = canonical_rotate(tets)
+    if t.shape[0] == 0:
+        return t.reshape(0, 4)
+    order = np.lexsort((t[:, 3], t[:, 2], t[:, 1], t[:, 0]))
+    return t[order]
+
+
+def fnv1a_order(order: np.ndarray) -> int:
+    """The reference's spatial-sort hash (4 low bytes of each index), tests/test_spatial_sort.cpp:46-51."""
+    h = 1469598103934665603
+    for v in np.asarray(order, dtype=np.int64).tolist():
+        v &= 0xFFFFFFFFFFFFFFFF
+        for b in range(4):
+            h ^= (v >> (8 * b)) & 0xFF
+            h = (h * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def fnv1a_cells(cells: np.ndarray) -> int:
+    """The reference's cell-sequence hash, tests/test_delaunay.cpp:44-56."""
+    h = 1469598103934665603
+
+    def mix(v: int) -> None:
+        nonlocal h
+        v &= 0xFFFFFFFFFFFFFFFF
+        for b in range(8):
+            h ^= (v >> (8 * b)) & 0xFF
+            h = (h * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+
+    c = np.asarray(cells, dtype=np.int64).reshape(-1, 4)
+    mix(c.shape[0])
+    for v in c.ravel().tolist():
+        mix(v)
+    return h
+
+
+# ---- the reference's test point sets -------------------------------------------
+
+def _ps(fn, *args) -> np.ndarray:
+    n = fn(*args, None)
+    out = np.zeros((n, 3), dtype=np.float64)
+    if n:
+        fn(*args, _ptr(out))
+    return out
+
+
+def ps_cylinder(n: int, q: int = 32, seed: int = 1) -> np.ndarray:
+    return _ps(ref().ps_cylinder, n, q, seed)
+
+
+def ps_sphere(n: int, q: int = 32, seed: int = 2) -> np.ndarray:
+    return _ps(ref().ps_sphere, n, q, seed)
+
+
+def ps_torus(n: int, q: int = 32, seed: int = 3) -> np.ndarray:
+    return _ps(ref().ps_torus, n, q, seed)
+
+
+def ps_box_shell(m: int) -> np.ndarray:
+    return _ps(ref().ps_box_shell, m)
+
+
+def ps_lattice(nx: int, ny: int, nz: int) -> np.ndarray:
+    return _ps(ref().ps_lattice, nx, ny, nz)
+
+
+def ps_random_cube(n: int, seed: int = 4) -> np.ndarray:
+    return _ps(ref().ps_random_cube, n, seed)
+
+
+def ps_rng_below(seed: int, m: int, count: int) -> np.ndarray:
+    out = np.zeros(count, dtype=np.int64)
+    ref().ps_rng_below(seed, m, count, _ptr(out))
+    return out

@@ -1,0 +1,77 @@
+"""The device build vs the reference compiled from source and the oracle:
+canonical tet sets bit-exact, vertex counts, all_cells, incident_cells."""
+import numpy as np
+import pytest
+
+import del3d_b200 as d3
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "random5": lambda: oracle.ps_random_cube(5, 4),
+    "random8": lambda: oracle.ps_random_cube(8, 4),
+    "random20": lambda: oracle.ps_random_cube(20, 4),
+    "random100": lambda: oracle.ps_random_cube(100, 4),
+    "random500": lambda: oracle.ps_random_cube(500, 4),
+    "lattice5": lambda: oracle.ps_lattice(5, 5, 5),
+    "plane_apex": lambda: np.array([[i, j, 0.0] for i in range(6) for j in range(6)] + [[2.0, 2.0, 3.0]]),
+    "box5": lambda: oracle.ps_box_shell(5),
+    "cylinder": lambda: oracle.ps_cylinder(300),
+    "sphere": lambda: oracle.ps_sphere(300),
+    "torus": lambda: oracle.ps_torus(300),
+    "lattice12": lambda: oracle.ps_lattice(12, 12, 12),
+    "uniform20k": lambda: d3.gen_uniform(20000, 1),
+    "sphere_q1024": lambda: d3.gen_sphere(20000, 5),
+    "clusters": lambda: d3.gen_clusters(20000, 7),
+}
+
+
+def reference(pts):
+    r = oracle.ref_build(pts)
+    return r, oracle.canonical_cells(r["cells"]), oracle.canonical_cells(r["all"])
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_cells_match_reference(cuda, case):
+    pts = CASES[case]()
+    r, cells, allc = reference(pts)
+    d = d3.Delaunay()
+    d.build(pts)
+    assert d.number_of_vertices() == r["n_vertices"]
+    got = d.finite_cells()
+    assert got.shape == cells.shape and (got == cells).all()
+    assert d.all_cells().shape == allc.shape and (d.all_cells() == allc).all()
+    # incident_cells agrees with finite_cells (tests/test_delaunay.cpp:141-159).
+    inc = d.incident_cells()
+    want = [[] for _ in range(len(pts))]
+    for ci, t in enumerate(got.tolist()):
+        for v in t:
+            want[v].append(ci)
+    assert all(list(a) == b for a, b in zip(inc, want))
+
+
+def test_deterministic(cuda):
+    pts = d3.gen_uniform(50000, 9)
+    a, b = d3.Delaunay(), d3.Delaunay()
+    a.build(pts)
+    b.build(pts)
+    assert (a.finite_cells() == b.finite_cells()).all()
+
+
+@pytest.mark.parametrize("pts", [np.zeros((0, 3)), np.zeros((1, 3)), np.array([[0, 0, 0], [1, 0, 0.0]]),
+                                 np.tile([1.0, 2.0, 3.0], (20, 1)),
+                                 np.array([[i, 2.0 * i, 3.0 * i] for i in range(10)]),
+                                 np.array([[i, j, 0.0] for i in range(5) for j in range(5)])])
+def test_degenerate_inputs_have_no_cells(cuda, pts):
+    d = d3.Delaunay()
+    d.build(pts)
+    assert d.finite_cells().shape[0] == 0
+    assert d.number_of_vertices() == len({tuple(p) for p in pts.tolist()})
+
+
+def test_non_finite_rejected(cuda):
+    pts = d3.gen_uniform(100, 1)
+    pts[17, 1] = np.nan
+    with pytest.raises(d3.Del3dError):
+        d3.Delaunay().build(pts)
