@@ -55,18 +55,30 @@ class Del3dError(RuntimeError):
         super().__init__(msg)
 
 
+class BuildStats(ctypes.Structure):
+    """What a build did (d3g_build_stats)."""
+    _fields_ = [("rounds", _I32), ("attempts", _I64), ("region_tets", _I64),
+                ("boundary_facets", _I64), ("ms_order", ctypes.c_double),
+                ("ms_rounds", ctypes.c_double), ("ms_output", ctypes.c_double),
+                ("ms_cavity", ctypes.c_double), ("ms_check", ctypes.c_double),
+                ("ms_restar", ctypes.c_double), ("launches_cavity", _I64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class _Result(ctypes.Structure):
     _fields_ = [
         ("n_points", _I64), ("n_vertices", _I64), ("n_cells", _I64),
         ("cells", ctypes.POINTER(_I32)), ("n_all", _I64), ("all_cells", ctypes.POINTER(_I32)),
         ("incident_offsets", ctypes.POINTER(_I64)), ("incident", ctypes.POINTER(_I32)),
-        ("rounds", _I32), ("n_exact", _I64), ("device_ms", ctypes.c_double),
+        ("device_ms", ctypes.c_double), ("stats", BuildStats),
     ]
 
 
 class _Options(ctypes.Structure):
     _fields_ = [("want_all_cells", _I32), ("want_incident", _I32), ("chunk", _I32),
-                ("max_rounds", _I32)]
+                ("max_rounds", _I32), ("timing", _I32)]
 
 
 class _PredStats(ctypes.Structure):
@@ -98,10 +110,13 @@ def library() -> ctypes.CDLL:
     lib.d3g_spatial_sort_device.argtypes = [_P, _I64, _P, _P]
     lib.d3g_shuffle_device.argtypes = [_I64, _P, _P]
     lib.d3g_options_default.argtypes = [ctypes.POINTER(_Options)]
+    lib.d3g_release_cached_memory.argtypes = []
+    lib.d3g_release_cached_memory.restype = _INT
     lib.d3g_build.argtypes = [_P, _I64, ctypes.POINTER(_Options), ctypes.POINTER(_Result)]
     lib.d3g_result_free.argtypes = [ctypes.POINTER(_Result)]
     lib.d3g_build_device.argtypes = [_P, _I64, ctypes.POINTER(_Options), _P, _I64,
-                                     ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P]
+                                     ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P,
+                                     ctypes.POINTER(BuildStats)]
     lib.d3g_gen_uniform.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, _P]
     lib.d3g_gen_sphere.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, _I32, _P]
     lib.d3g_gen_clusters.argtypes = [_I64, ctypes.c_uint32, _I32, ctypes.c_double, _P]
@@ -265,8 +280,9 @@ class Delaunay:
         self._n_vertices = 0
         self.rounds = 0
         self.device_ms = 0.0
+        self.stats = {}
 
-    def build(self, points, chunk: int = 0) -> None:
+    def build(self, points, chunk: int = 0, all_cells: bool = True, incident: bool = True) -> None:
         """Builds the triangulation.  Points equal to an earlier point are
         ignored; a repeated point is reported under the index of its copy that
         comes last in the spatial-sort order, as in the reference."""
@@ -275,6 +291,8 @@ class Delaunay:
         opts = _Options()
         lib.d3g_options_default(ctypes.byref(opts))
         opts.chunk = int(chunk)
+        opts.want_all_cells = int(all_cells)
+        opts.want_incident = int(incident)
         res = _Result()
         _check(lib.d3g_build(_ptr(pts), pts.shape[0], ctypes.byref(opts), ctypes.byref(res)), "build")
         try:
@@ -289,7 +307,8 @@ class Delaunay:
             self._inc = (np.ctypeslib.as_array(res.incident, shape=(ninc,)).copy()
                          if ninc else np.zeros(0, dtype=np.int32))
             self._n_vertices = int(res.n_vertices)
-            self.rounds = int(res.rounds)
+            self.stats = res.stats.as_dict()
+            self.rounds = int(res.stats.rounds)
             self.device_ms = float(res.device_ms)
         finally:
             lib.d3g_result_free(ctypes.byref(res))
@@ -315,25 +334,31 @@ class Delaunay:
         return self._n_vertices
 
 
-def build_device(points_dev, cap_cells: Optional[int] = None, stream: int = 0, chunk: int = 0):
-    """Builds from a device-resident torch tensor (n, 3) float64; returns the
-    canonical finite cells as a device int32 tensor (n_cells, 4) and the vertex
-    count.  Synchronises `stream`."""
+def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: bool = False,
+                 stats: Optional[dict] = None):
+    """Builds from a device-resident torch tensor (n, 3) float64 on `stream`
+    (a raw cudaStream_t handle; 0 = default) and returns the canonical finite
+    cells as a device int32 tensor view (n_cells, 4) and the vertex count.
+    `out` may supply the (cap, 4) int32 output buffer.  Synchronises `stream`."""
     import torch
 
     lib = library()
     assert points_dev.is_cuda and points_dev.dtype == torch.float64
     x = points_dev.contiguous()
     n = x.shape[0]
-    if cap_cells is None:
-        cap_cells = 8 * n + 64
-    out = torch.empty((cap_cells, 4), dtype=torch.int32, device=x.device)
+    if out is None:
+        out = torch.empty((8 * n + 64, 4), dtype=torch.int32, device=x.device)
     nc, nv = _I64(0), _I64(0)
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
     opts.chunk = int(chunk)
-    _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), cap_cells,
-                                ctypes.byref(nc), ctypes.byref(nv), _P(stream)), "build_device")
+    opts.timing = int(timing)
+    st = BuildStats()
+    _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), out.shape[0],
+                                ctypes.byref(nc), ctypes.byref(nv), _P(stream), ctypes.byref(st)),
+           "build_device")
+    if stats is not None:
+        stats.update(st.as_dict())
     return out[: nc.value], nv.value
 
 

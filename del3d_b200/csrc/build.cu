@@ -47,6 +47,7 @@ namespace {
 constexpr int kInf = -1;
 constexpr int kWalkLimit = 1 << 20;
 constexpr int kRotateLimit = 1 << 16;
+constexpr int kRoundsPerBatch = 16;
 
 enum : int { WS_DONE = 0, WS_CAND = 1, WS_LOST = 2, WS_WIN = 3, WS_OVERFLOW = 4, WS_FAIL = 5 };
 
@@ -103,11 +104,39 @@ struct Workers {
 };
 
 struct Round {
-    unsigned long long tag;   // (~round) << 32: newer rounds win every stale claim
+    const unsigned* round;    // current round number (device), set by k_round_begin
     int skip[4];              // the initial tet's vertices (already inserted)
     int* counters;            // [0] active workers, [1] overflowed workers, [2] winners
+    unsigned long long* sums; // [0] region tets, [1] boundary facets of the winners
+    unsigned long long* totals; // [0] winners, [1] attempts, [2] rounds with work,
+                                // [3] overflow seen, [4] stalled round seen, [5] active
     uint32_t* status;
 };
+
+/// Claim key of point v this round: (~round) << 32 makes every newer round win
+/// against stale claims; the point rank breaks ties (earliest wins).
+__device__ __forceinline__ unsigned long long claim_key(const Round& R, int v) {
+    return ((unsigned long long)(0xFFFFFFFFu - *R.round) << 32) |
+           (unsigned long long)(uint32_t(v)) << 1;
+}
+
+__global__ void k_round_begin(Round R) {
+    unsigned* r = const_cast<unsigned*>(R.round);
+    *r += 1;
+    R.counters[0] = R.counters[1] = R.counters[2] = 0;
+}
+
+/// Folds one round's counters into the running totals; flags a round in which
+/// workers were active but nobody won (the earliest pending point must win).
+__global__ void k_round_end(Round R) {
+    const int active = R.counters[0], over = R.counters[1], won = R.counters[2];
+    R.totals[0] += (unsigned long long)won;
+    R.totals[1] += (unsigned long long)(active + won);
+    if (active + won > 0) R.totals[2] += 1;
+    if (over > 0) R.totals[3] = 1;
+    if (active > 0 && won == 0 && over == 0) R.totals[4] = 1;
+    R.totals[5] = (unsigned long long)active;
+}
 
 /// orient3d of tet (q0,q1,q2,q3) with vertex i replaced by p.
 __device__ __forceinline__ int orient_replaced(const Pt* q, int i, const Pt& p, uint32_t* st) {
@@ -205,7 +234,7 @@ __device__ int next_point(const Workers& W, int w, const int* skip) {
 /// One warp per worker: locate the worker's point, then grow its conflict
 /// region breadth-first, eight region tets (32 facets) per step, claiming
 /// every region tet (key) and every tet across the region boundary (key|1).
-__global__ void __launch_bounds__(128) k_cavity(Tables T, Workers W, Round R, const double* __restrict__ vx,
+__global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R, const double* __restrict__ vx,
                                                 int first) {
     const int lane = threadIdx.x & 31;
     const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -222,7 +251,7 @@ __global__ void __launch_bounds__(128) k_cavity(Tables T, Workers W, Round R, co
         if (lane == 0) W.state[w] = WS_FAIL;
         return;
     }
-    const unsigned long long key = R.tag | (unsigned long long)(uint32_t(v)) << 1;
+    const unsigned long long key = claim_key(R, v);
     const unsigned long long mine = key >> 1;
     int* cav = W.cav + int64_t(w) * W.cav_cap;
     int* fac = W.fac + int64_t(w) * W.fac_cap;
@@ -304,12 +333,12 @@ __global__ void __launch_bounds__(128) k_cavity(Tables T, Workers W, Round R, co
 }
 
 /// One warp per candidate: it wins if it still holds every claim it made.
-__global__ void __launch_bounds__(128) k_check(Tables T, Workers W, Round R, int first) {
+__global__ void __launch_bounds__(128, 8) k_check(Tables T, Workers W, Round R, int first) {
     const int lane = threadIdx.x & 31;
     const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (w >= W.n || W.state[w] != WS_CAND) return;
     const int v = W.cur[w];
-    const unsigned long long key = R.tag | (unsigned long long)(uint32_t(v)) << 1;
+    const unsigned long long key = claim_key(R, v);
     const int* cav = W.cav + int64_t(w) * W.cav_cap;
     const int* fac = W.fac + int64_t(w) * W.fac_cap;
     const int ncav = W.ncav[w], nfac = W.nfac[w];
@@ -324,7 +353,7 @@ __global__ void __launch_bounds__(128) k_check(Tables T, Workers W, Round R, int
 }
 
 /// One warp per winner: re-star its region, one boundary facet per lane.
-__global__ void __launch_bounds__(128) k_restar(Tables T, Workers W, Round R, int first) {
+__global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R, int first) {
     __shared__ int sh_count[2];
     const int lane = threadIdx.x & 31;
     const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -335,7 +364,7 @@ __global__ void __launch_bounds__(128) k_restar(Tables T, Workers W, Round R, in
     const int v = exists ? W.cur[w] : -1;
     bool advanced = false;
     if (state == WS_WIN) {
-        const unsigned long long key = R.tag | (unsigned long long)(uint32_t(v)) << 1;
+        const unsigned long long key = claim_key(R, v);
         const int* cav = W.cav + int64_t(w) * W.cav_cap;
         const int* fac = W.fac + int64_t(w) * W.fac_cap;
         int4* sv = W.st_v + int64_t(w) * W.fac_cap;
@@ -424,6 +453,10 @@ __global__ void __launch_bounds__(128) k_restar(Tables T, Workers W, Round R, in
             }
             for (int k = F + lane; k < C; k += 32) T.alive[cav[k]] = 0;
             advanced = true;
+            if (lane == 0) {
+                atomicAdd(R.sums, (unsigned long long)C);
+                atomicAdd(R.sums + 1, (unsigned long long)F);
+            }
         }
     }
     if (lane == 0 && exists) {
@@ -707,14 +740,14 @@ struct DeviceResult {
     DevBuf<int64_t> inc_off;
     DevBuf<int32_t> inc;
     int64_t n_cells = 0, n_all = 0, n_vertices = 0, n_inc = 0;
-    int rounds = 0;
+    d3g_build_stats stats{};
     void reset() {
         cells.release();
         all.release();
         inc_off.release();
         inc.release();
         n_cells = n_all = n_vertices = n_inc = 0;
-        rounds = 0;
+        stats = d3g_build_stats{};
     }
 };
 
@@ -745,6 +778,40 @@ int sort_cells(DevBuf<int4>& cells, DevBuf<unsigned long long>& khi, DevBuf<unsi
 }  // namespace
 
 int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
+                      DeviceResult& R);
+
+/// A non-blocking stream of the calling thread for the current device; it lives
+/// as long as the thread, so buffers bound to it can be freed at any later time.
+cudaStream_t internal_stream() {
+    thread_local cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
+        streams[dev] = nullptr;
+    return streams[dev];
+}
+
+/// Runs the build on `s`, or - for the legacy default stream, which cannot be
+/// captured into a graph - on the thread's internal stream, after the legacy
+/// stream's prior work (the build synchronises its stream before returning).
+int build_on_stream(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
+                    DeviceResult& R) {
+    D3G_TRY(prepare_device());
+    if (s != nullptr && s != cudaStreamLegacy) return build_device_impl(d_xyz, n, opt, s, R);
+    cudaStream_t own = internal_stream();
+    if (!own) {
+        set_error("d3g_build: could not create a stream");
+        return D3G_ERR_CUDA;
+    }
+    cudaEvent_t ev;
+    D3G_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaEventRecord(ev, cudaStreamLegacy);
+    cudaStreamWaitEvent(own, ev, 0);
+    cudaEventDestroy(ev);
+    return build_device_impl(d_xyz, n, opt, own, R);
+}
+
+int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
                       DeviceResult& R) {
     R.reset();
     if (n == 0) return D3G_OK;
@@ -758,6 +825,15 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     D3G_CUDA(cudaMemsetAsync(status.p, 0, 4 * sizeof(uint32_t), s));
     k_check_finite<<<grid_for(3 * n, 256), 256, 0, s>>>(d_xyz, 3 * n, status.p + 1);
 
+    cudaEvent_t ph[4];
+    for (auto& e : ph) cudaEventCreate(&e);
+    struct PhGuard {
+        cudaEvent_t* e;
+        ~PhGuard() {
+            for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
+        }
+    } ph_guard{ph};
+    cudaEventRecord(ph[0], s);
     // ---- insertion order and duplicate groups ----
     DevBuf<int32_t> order;
     D3G_TRY(order.alloc(size_t(N), s));
@@ -811,6 +887,7 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         return D3G_ERR_INVALID_INPUT;
     }
 
+    cudaEventRecord(ph[1], s);
     // ---- the first tet: the first four affinely independent vertices ----
     int v2 = -1, v3 = -1;
     if (nv >= 4) {
@@ -871,14 +948,29 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     k_init_tets<<<1, 32, 0, s>>>(T, vx.p, 0, 1, v2, v3, status.p);
 
     // ---- workers ----
-    const int chunk = opt.chunk > 0 ? opt.chunk : 64;
+    // A level of s points goes into a triangulation of p earlier points.  Two
+    // insertions collide when their regions (about 20 tets and their ring)
+    // meet, so the useful number of simultaneous insertions grows with p, not
+    // with s: each level gets about p / alpha workers (a fixed chunk if the
+    // caller asks for one), each with a chunk of at least kMinChunk points.
+    const int alpha = opt.chunk < 0 ? -opt.chunk : 48;
+    constexpr int kMinChunk = 16;
     int64_t hb[64];
     const int nb = multiscale_bounds(nv, hb, 63);
+    auto level_chunk = [&](int64_t lb, int64_t le) -> int {
+        if (opt.chunk > 0) return opt.chunk;
+        const int64_t s_ = le - lb;
+        int64_t w_ = std::max<int64_t>(1, lb / alpha);
+        w_ = std::min<int64_t>(w_, (s_ + kMinChunk - 1) / kMinChunk);
+        return int((s_ + w_ - 1) / w_);
+    };
     int maxw = 1;
     for (int k = 0; k < nb; ++k) {
         const int64_t lo = (k + 1 < nb) ? hb[k + 1] : 0;
         const int64_t cnt = hb[k] - lo;
-        maxw = std::max<int64_t>(maxw, (cnt + chunk - 1) / chunk);
+        if (cnt <= 0) continue;
+        const int ch = level_chunk(lo, hb[k]);
+        maxw = std::max<int64_t>(maxw, (cnt + ch - 1) / ch);
     }
     Workers W;
     W.cav_cap = 256;
@@ -901,6 +993,14 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     D3G_TRY(wsv.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(wsn.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(counters.alloc(3, s));
+    DevBuf<unsigned long long> sums, totals;
+    DevBuf<unsigned> dround;
+    D3G_TRY(sums.alloc(2, s));
+    D3G_TRY(totals.alloc(6, s));
+    D3G_TRY(dround.alloc(1, s));
+    D3G_CUDA(cudaMemsetAsync(sums.p, 0, 2 * sizeof(unsigned long long), s));
+    D3G_CUDA(cudaMemsetAsync(totals.p, 0, 6 * sizeof(unsigned long long), s));
+    D3G_CUDA(cudaMemsetAsync(dround.p, 0, sizeof(unsigned), s));
     W.cur = wcur.p;
     W.end = wend.p;
     W.beg = wbeg.p;
@@ -922,10 +1022,23 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     Rd.skip[2] = v2;
     Rd.skip[3] = v3;
     Rd.counters = counters.p;
+    Rd.sums = sums.p;
+    Rd.totals = totals.p;
+    Rd.round = dround.p;
     Rd.status = status.p;
     const int max_rounds = opt.max_rounds > 0 ? opt.max_rounds : (1 << 20);
     int round = 0;
     const bool trace = getenv("D3G_TRACE") != nullptr;
+    cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (opt.timing)
+        for (auto& e : kev) cudaEventCreate(&e);
+    struct EvGuard {
+        cudaEvent_t* e;
+        ~EvGuard() {
+            for (int i = 0; i < 4; ++i)
+                if (e[i]) cudaEventDestroy(e[i]);
+        }
+    } ev_guard{kev};
     // Levels from the coarsest ([0, hb[nb-1])) to the finest ([hb[1], hb[0])).
     for (int k = nb - 1; k >= 0; --k) {
         const int lb = int(k + 1 < nb ? hb[k + 1] : 0);
@@ -933,9 +1046,18 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         const int plb = int(k + 2 < nb ? hb[k + 2] : 0);
         const int ple = lb;
         if (le <= lb) continue;
+        const int chunk = level_chunk(lb, le);
         W.n = (le - lb + chunk - 1) / chunk;
         const int round0 = round;
         long long won = 0, attempts = 0;
+        long long won_before = 0, att_before = 0;
+        {
+            unsigned long long ht0[2];
+            D3G_CUDA(cudaMemcpyAsync(ht0, totals.p, sizeof ht0, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaStreamSynchronize(s));
+            won_before = (long long)ht0[0];
+            att_before = (long long)ht0[1];
+        }
         cudaEvent_t ev0 = nullptr, ev1 = nullptr;
         if (trace) {
             cudaEventCreate(&ev0);
@@ -944,20 +1066,52 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         }
         k_setup_level<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, lb, le, chunk, plb, ple,
                                                                   make_int4(0, 1, v2, v3));
+        const unsigned g = unsigned((int64_t(W.n) * 32 + 127) / 128);
+        auto one_round = [&](bool timed) {
+            k_round_begin<<<1, 1, 0, s>>>(Rd);
+            if (timed) cudaEventRecord(kev[0], s);
+            k_cavity<<<g, 128, 0, s>>>(T, W, Rd, vx.p, 0);
+            if (timed) cudaEventRecord(kev[1], s);
+            k_check<<<g, 128, 0, s>>>(T, W, Rd, 0);
+            if (timed) cudaEventRecord(kev[2], s);
+            k_restar<<<g, 128, 0, s>>>(T, W, Rd, 0);
+            if (timed) cudaEventRecord(kev[3], s);
+            k_round_end<<<1, 1, 0, s>>>(Rd);
+        };
+        // Rounds go out in batches captured as one CUDA graph; the host looks at
+        // the counters once per batch.  Rounds after the level is done find no
+        // active worker and return at once.
+        cudaGraphExec_t gexec = nullptr;
+        if (!opt.timing) {
+            cudaGraph_t graph = nullptr;
+            D3G_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            for (int r = 0; r < kRoundsPerBatch; ++r) one_round(false);
+            D3G_CUDA(cudaStreamEndCapture(s, &graph));
+            const cudaError_t ge = cudaGraphInstantiate(&gexec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ge != cudaSuccess) {
+                set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ge));
+                return D3G_ERR_CUDA;
+            }
+        }
+        struct GraphGuard {
+            cudaGraphExec_t* g;
+            ~GraphGuard() {
+                if (*g) cudaGraphExecDestroy(*g);
+            }
+        } graph_guard{&gexec};
         for (;;) {
-            if (++round > max_rounds) {
+            const int batch = opt.timing ? 1 : kRoundsPerBatch;
+            round += batch;
+            if (round > max_rounds) {
                 set_error("d3g_build: insertion round limit reached");
                 return D3G_ERR_ROUND_LIMIT;
             }
-            Rd.tag = (unsigned long long)(0xFFFFFFFFu - uint32_t(round)) << 32;
-            D3G_CUDA(cudaMemsetAsync(counters.p, 0, 3 * sizeof(int), s));
-            const unsigned g = unsigned((int64_t(W.n) * 32 + 127) / 128);
-            k_cavity<<<g, 128, 0, s>>>(T, W, Rd, vx.p, 0);
-            k_check<<<g, 128, 0, s>>>(T, W, Rd, 0);
-            k_restar<<<g, 128, 0, s>>>(T, W, Rd, 0);
-            int hc[3] = {0, 0, 0};
+            if (opt.timing) one_round(true);
+            else D3G_CUDA(cudaGraphLaunch(gexec, s));
+            unsigned long long ht[6];
             uint32_t hs = 0;
-            D3G_CUDA(cudaMemcpyAsync(hc, counters.p, sizeof hc, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaMemcpyAsync(ht, totals.p, sizeof ht, cudaMemcpyDeviceToHost, s));
             D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
             D3G_CUDA(cudaStreamSynchronize(s));
             if (hs != 0) {
@@ -965,17 +1119,27 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
                 if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");
                 return st;
             }
-            if (hc[1] > 0) {
+            if (ht[3]) {
                 set_error("d3g_build: a conflict region exceeded the per-worker scratch");
                 return D3G_ERR_CAVITY_CAPACITY;
             }
-            won += hc[2];
-            attempts += hc[0] + hc[2];
-            if (hc[0] == 0) break;
-            if (hc[2] == 0) {   // the earliest pending point must always win
+            if (ht[4]) {
                 set_error("d3g_build: an insertion round made no progress");
                 return D3G_ERR_INTERNAL;
             }
+            if (opt.timing) {
+                float a = 0.f, b2 = 0.f, c = 0.f;
+                cudaEventElapsedTime(&a, kev[0], kev[1]);
+                cudaEventElapsedTime(&b2, kev[1], kev[2]);
+                cudaEventElapsedTime(&c, kev[2], kev[3]);
+                R.stats.ms_cavity += a;
+                R.stats.ms_check += b2;
+                R.stats.ms_restar += c;
+                R.stats.launches_cavity += 1;
+            }
+            won = (long long)ht[0] - won_before;
+            attempts = (long long)ht[1] - att_before;
+            if (ht[5] == 0) break;
         }
         if (trace) {
             cudaEventRecord(ev1, s);
@@ -988,7 +1152,16 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
             cudaEventDestroy(ev1);
         }
     }
-    R.rounds = round;
+    {
+        unsigned long long hs2[2] = {0, 0}, ht[6];
+        D3G_CUDA(cudaMemcpyAsync(hs2, sums.p, sizeof hs2, cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaMemcpyAsync(ht, totals.p, sizeof ht, cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));
+        R.stats.region_tets = int64_t(hs2[0]);
+        R.stats.boundary_facets = int64_t(hs2[1]);
+        R.stats.rounds = int(ht[2]);
+        R.stats.attempts = int64_t(ht[1]);
+    }
     // Release round scratch before the output stage.
     wcav.release();
     wfac.release();
@@ -997,6 +1170,7 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     claim.release();
     fnew.release();
 
+    cudaEventRecord(ph[2], s);
     // ---- output: canonical cells ----
     int ntet = 0;
     D3G_CUDA(cudaMemcpyAsync(&ntet, tet_count.p, sizeof ntet, cudaMemcpyDeviceToHost, s));
@@ -1052,8 +1226,18 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         R.n_inc = m;
     }
     D3G_CUDA(cudaGetLastError());
+    cudaEventRecord(ph[3], s);
     D3G_CUDA(cudaMemcpyAsync(hst, status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     D3G_CUDA(cudaStreamSynchronize(s));
+    {
+        float a = 0.f, b = 0.f, c = 0.f;
+        cudaEventElapsedTime(&a, ph[0], ph[1]);
+        cudaEventElapsedTime(&b, ph[1], ph[2]);
+        cudaEventElapsedTime(&c, ph[2], ph[3]);
+        R.stats.ms_order = a;
+        R.stats.ms_rounds = b;
+        R.stats.ms_output = c;
+    }
     return status_from_bits(hst[0]);
 }
 
@@ -1069,6 +1253,7 @@ void d3g_options_default(d3g_options* o) {
     o->want_incident = 1;
     o->chunk = 0;
     o->max_rounds = 0;
+    o->timing = 0;
 }
 
 void d3g_result_free(d3g_result* r) {
@@ -1103,14 +1288,14 @@ int d3g_build(const double* xyz, int64_t n, const d3g_options* opts, d3g_result*
         D3G_TRY(dx.alloc(size_t(3 * n), s));
         D3G_CUDA(cudaMemcpyAsync(dx.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
         cudaEventRecord(e0, s);
-        st = build_device_impl(dx.p, n, o, s, R);
+        st = build_on_stream(dx.p, n, o, s, R);
         cudaEventRecord(e1, s);
     }
     if (st == D3G_OK) {
         out->n_vertices = R.n_vertices;
         out->n_cells = R.n_cells;
         out->n_all = R.n_all;
-        out->rounds = R.rounds;
+        out->stats = R.stats;
         out->cells = static_cast<int32_t*>(malloc(sizeof(int32_t) * 4 * size_t(R.n_cells > 0 ? R.n_cells : 1)));
         if (R.n_cells > 0)
             cudaMemcpyAsync(out->cells, R.cells.p, sizeof(int4) * R.n_cells, cudaMemcpyDeviceToHost, s);
@@ -1144,7 +1329,8 @@ int d3g_build(const double* xyz, int64_t n, const d3g_options* opts, d3g_result*
 }
 
 int d3g_build_device(const double* d_xyz, int64_t n, const d3g_options* opts, int32_t* d_cells,
-                     int64_t cap_cells, int64_t* n_cells_out, int64_t* n_vertices_out, void* stream) {
+                     int64_t cap_cells, int64_t* n_cells_out, int64_t* n_vertices_out, void* stream,
+                     d3g_build_stats* stats) {
     if (n < 0 || (n > 0 && !d_xyz) || cap_cells < 0) return D3G_ERR_INVALID_ARGUMENT;
     d3g_options o;
     d3g_options_default(&o);
@@ -1153,10 +1339,11 @@ int d3g_build_device(const double* d_xyz, int64_t n, const d3g_options* opts, in
     o.want_incident = 0;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     DeviceResult R;
-    const int st = build_device_impl(d_xyz, n, o, s, R);
+    const int st = build_on_stream(d_xyz, n, o, s, R);
     if (st != D3G_OK) return st;
     if (n_cells_out) *n_cells_out = R.n_cells;
     if (n_vertices_out) *n_vertices_out = R.n_vertices;
+    if (stats) *stats = R.stats;
     if (R.n_cells > cap_cells) {
         set_error("d3g_build_device: output capacity too small");
         return D3G_ERR_INVALID_ARGUMENT;

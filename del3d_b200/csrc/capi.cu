@@ -3,6 +3,7 @@
 #include "common.cuh"
 
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -39,6 +40,31 @@ int ensure_device() {
         cudaGetLastError();
         return D3G_ERR_NO_DEVICE;
     }
+    return prepare_device();
+}
+
+int prepare_device() {
+    // The build allocates and frees gigabytes per call from the stream-ordered
+    // pool; keep that memory in the pool instead of handing it back to the
+    // driver at every synchronisation (d3g_release_cached_memory trims it).
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("no current CUDA device");
+        return D3G_ERR_NO_DEVICE;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && !done[dev]) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t thr = ~uint64_t(0);
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        cudaGetLastError();
+        done[dev] = true;
+    }
     return D3G_OK;
 }
 
@@ -66,6 +92,15 @@ const char* d3g_status_string(int status) {
 }
 
 const char* d3g_last_error(void) { return g_last_error.c_str(); }
+
+int d3g_release_cached_memory(void) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return D3G_ERR_NO_DEVICE;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return D3G_ERR_CUDA;
+    if (cudaDeviceSynchronize() != cudaSuccess) return D3G_ERR_CUDA;
+    return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? D3G_OK : D3G_ERR_CUDA;
+}
 
 int d3g_predicate_arity(int kind) {
     switch (kind) {

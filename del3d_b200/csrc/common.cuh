@@ -73,7 +73,9 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = int64_t(kNumSMs) * 
     return unsigned(g);
 }
 
-/// Ensures a CUDA device is present and current.
+/// Ensures a CUDA device is present and current, and prepares it.
 int ensure_device();
+/// Once per device: keeps freed stream-ordered allocations cached in the pool.
+int prepare_device();
 
 }  // namespace d3g

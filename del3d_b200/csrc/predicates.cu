@@ -187,6 +187,7 @@ int predicates_device(const double* d_pts, int64_t n_pts, const int32_t* d_idx, 
         if (stats) *stats = d3g_predicate_stats{0, 0};
         return D3G_OK;
     }
+    D3G_TRY(prepare_device());
     if (!d_pts || !d_idx || !d_out) {
         set_error("d3g_predicates: null pointer");
         return D3G_ERR_INVALID_ARGUMENT;

@@ -52,6 +52,11 @@ const char* d3g_status_string(int status);
 /* Detail of the last error on the calling thread ("" if none). */
 const char* d3g_last_error(void);
 
+/* The library keeps device memory it frees cached in the current device's
+ * stream-ordered pool (builds allocate gigabytes per call).  This returns the
+ * cached memory to the driver; it synchronises the device. */
+int d3g_release_cached_memory(void);
+
 /* ---- predicates ------------------------------------------------------------
  * Batch evaluation over index tuples into a point table `pts` (3 doubles per
  * point, x y z).  `idx` holds k int32 indices per query, k given by the kind;
@@ -96,10 +101,36 @@ int d3g_orient2d(const double* six, int64_t n_queries, int8_t* sign_out);
  * median splits), bit for bit: order[k] = index of the k-th point. */
 int d3g_spatial_sort(const double* xyz, int64_t n, int32_t* order);
 int d3g_spatial_sort_device(const double* d_xyz, int64_t n, int32_t* d_order, void* stream);
+/* The first stage alone: the rand48 Fisher-Yates shuffle of 0..n-1
+ * (reference src/rand48.h:146-153 with the engine seeded to 1). */
+int d3g_shuffle_device(int64_t n, int32_t* d_order, void* stream);
 
 /* ---- the build ---------------------------------------------------------------
  * A d3g_result holds one triangulation on the host.  It owns its arrays; free
  * it with d3g_result_free.  Fields are valid until then. */
+typedef struct d3g_options {
+    int32_t want_all_cells;  /* also produce all_cells                           */
+    int32_t want_incident;   /* also produce incident_cells                      */
+    int32_t chunk;           /* > 0: points per worker chunk; < 0: -alpha, one   */
+                             /* worker per alpha earlier points; 0 = default    */
+    int32_t max_rounds;      /* 0 = default                                      */
+    int32_t timing;          /* time each insertion kernel with CUDA events      */
+} d3g_options;
+
+/* What a build did (filled by d3g_build and d3g_build_device). */
+typedef struct d3g_build_stats {
+    int32_t rounds;          /* insertion rounds                                 */
+    int64_t attempts;        /* insertion attempts, winners and losers           */
+    int64_t region_tets;     /* sum over insertions of conflict-region tets      */
+    int64_t boundary_facets; /* sum over insertions of region boundary facets    */
+    double ms_order;         /* spatial order + duplicate grouping               */
+    double ms_rounds;        /* insertion rounds                                 */
+    double ms_output;        /* canonical output                                 */
+    /* with d3g_options.timing: device time of each insertion kernel, summed */
+    double ms_cavity, ms_check, ms_restar;
+    int64_t launches_cavity;
+} d3g_build_stats;
+
 typedef struct d3g_result {
     int64_t n_points;        /* input size                                       */
     int64_t n_vertices;      /* distinct points (number_of_vertices())           */
@@ -110,17 +141,9 @@ typedef struct d3g_result {
     int64_t* incident_offsets; /* n_points + 1 (CSR of incident_cells())         */
     int32_t* incident;       /* incident_offsets[n_points] finite-cell indices   */
     /* build statistics */
-    int32_t rounds;          /* insertion rounds                                 */
-    int64_t n_exact;         /* predicate calls that reached the exact stage     */
     double device_ms;        /* device time of the build (CUDA events)           */
+    d3g_build_stats stats;
 } d3g_result;
-
-typedef struct d3g_options {
-    int32_t want_all_cells;  /* also produce all_cells                           */
-    int32_t want_incident;   /* also produce incident_cells                      */
-    int32_t chunk;           /* points per worker chunk (0 = default)            */
-    int32_t max_rounds;      /* 0 = default                                      */
-} d3g_options;
 
 /* Fills `opts` with the defaults (all outputs on). */
 void d3g_options_default(d3g_options* opts);
@@ -135,14 +158,20 @@ void d3g_result_free(d3g_result* r);
  * cells into a caller-supplied device array of `cap_cells` x 4 int32 on
  * `stream`.  *n_cells_out receives the cell count (also when it exceeds
  * cap_cells, in which case nothing is written and D3G_ERR_INVALID_ARGUMENT is
- * returned).  Synchronises `stream`. */
+ * returned).  `stats` may be NULL.  Synchronises `stream`. */
 int d3g_build_device(const double* d_xyz, int64_t n, const d3g_options* opts, int32_t* d_cells,
                      int64_t cap_cells, int64_t* n_cells_out, int64_t* n_vertices_out,
-                     void* stream);
+                     void* stream, d3g_build_stats* stats);
 
 /* ---- synthetic inputs (host) -------------------------------------------------
  * Deterministic generators (std::mt19937 with u01 = word * 2^-32, written out). */
 void d3g_gen_uniform(int64_t n, uint32_t seed, double lo, double hi, double* xyz);
+/* Sphere of radius r (z and angle uniform), coordinates snapped to 1/q (q a power of two). */
+void d3g_gen_sphere(int64_t n, uint32_t seed, double r, int32_t q, double* xyz);
+/* k Gaussian clusters of standard deviation sigma, centres uniform in [0.1,0.9]^3. */
+void d3g_gen_clusters(int64_t n, uint32_t seed, int32_t k, double sigma, double* xyz);
+/* The first n points of the integer lattice of side ceil(n^(1/3)), lexicographic. */
+void d3g_gen_lattice(int64_t n, double* xyz);
 
 #ifdef __cplusplus
 }
