@@ -12,6 +12,8 @@
 // kernel per query.
 #include "common.cuh"
 
+#include <mutex>
+
 namespace d3g {
 namespace {
 
@@ -251,4 +253,122 @@ int orient2d_device(const double* d_six, int64_t nq, int8_t* d_out, cudaStream_t
     return status_from_bits(bits);
 }
 
+// ---- the entry point that allocates nothing ---------------------------------
+//
+// Some callers cannot allocate device memory when they evaluate predicates: a
+// framework whose caching allocator has reserved the whole device, or a code
+// path where an allocation's implicit synchronisation or possible failure is not
+// acceptable.  d3g_predicates_noalloc_device serves them: its exact-stage queue
+// and counters live in the fixed array below instead of stream-ordered
+// allocations.  The array exists once per device that loads this library and is
+// held until the process exits.
+
+namespace {
+
+struct NoAllocScratch {
+    unsigned long long counters[2];            // [0] status bits, [1] exact-stage queue length
+    int64_t queue[D3G_NOALLOC_MAX_QUERIES];     // indices of the queries the filter left uncertain
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+/// The device address of g_noalloc_scratch on the current device.  In host
+/// code the symbol is a host-side stand-in, not a device address, so it is
+/// looked up once per device (with that device current) and cached.
+int noalloc_scratch(NoAllocScratch** out) {
+    static std::mutex mu;
+    static NoAllocScratch* addr[64] = {};
+    int dev = 0;
+    const cudaError_t ge = cudaGetDevice(&dev);
+    if (ge != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        set_error("d3g_predicates_noalloc_device: no usable current device");
+        return D3G_ERR_NO_DEVICE;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            return D3G_ERR_CUDA;
+        }
+        addr[dev] = static_cast<NoAllocScratch*>(p);
+    }
+    *out = addr[dev];
+    return D3G_OK;
+}
+
+}  // namespace
+
+int predicates_noalloc_device(const double* d_pts, int64_t n_pts, const int32_t* d_idx, int64_t nq,
+                              int kind, int8_t* d_out, cudaStream_t stream,
+                              d3g_predicate_stats* stats) {
+    if (nq < 0 || n_pts < 0 || d3g_predicate_arity(kind) == 0) {
+        set_error("d3g_predicates_noalloc_device: bad size or kind");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    if (nq > D3G_NOALLOC_MAX_QUERIES) {
+        set_error("d3g_predicates_noalloc_device: at most D3G_NOALLOC_MAX_QUERIES (1048576) "
+                  "queries per call");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    if (nq == 0) {
+        if (stats) *stats = d3g_predicate_stats{0, 0};
+        return D3G_OK;
+    }
+    if (!d_pts || !d_idx || !d_out) {
+        set_error("d3g_predicates_noalloc_device: null pointer");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    if (kind == D3G_ORIENT3D && (reinterpret_cast<uintptr_t>(d_idx) & 15u) != 0) {
+        set_error("d3g_predicates_noalloc_device: orient3d index array must be 16-byte aligned");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    NoAllocScratch* sc = nullptr;
+    D3G_TRY(noalloc_scratch(&sc));
+    // The array keeps the previous call's contents: the counters must start at zero.
+    D3G_CUDA(cudaMemsetAsync(sc->counters, 0, sizeof sc->counters, stream));
+    uint32_t* status = reinterpret_cast<uint32_t*>(&sc->counters[0]);
+    unsigned long long* qcount = &sc->counters[1];
+    const int blk = 256;
+    if (kind == D3G_ORIENT3D || kind == D3G_IN_SPHERE || kind == D3G_IN_SPHERE_UNPERTURBED) {
+        const unsigned g = grid_for(nq, blk, int64_t(kNumSMs) * 16);
+        if (kind == D3G_ORIENT3D) {
+            k_filter_orient3d<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, sc->queue, qcount,
+                                                     status);
+            k_exact_orient3d<<<kNumSMs * 4, 256, 0, stream>>>(d_pts, d_idx, d_out, sc->queue, qcount,
+                                                             status);
+        } else {
+            k_filter_in_sphere<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, sc->queue,
+                                                      qcount, status);
+            k_exact_in_sphere<<<kNumSMs * 8, 128, 0, stream>>>(
+                d_pts, d_idx, d_out, sc->queue, qcount, kind == D3G_IN_SPHERE ? 1 : 0, status);
+        }
+    } else {
+        k_coplanar<<<grid_for(nq, 128), 128, 0, stream>>>(d_pts, n_pts, d_idx, nq, kind, d_out,
+                                                          qcount, status);
+    }
+    D3G_CUDA(cudaGetLastError());
+    unsigned long long host_counters[2] = {0, 0};
+    D3G_CUDA(cudaMemcpyAsync(host_counters, sc->counters, sizeof host_counters,
+                             cudaMemcpyDeviceToHost, stream));
+    D3G_CUDA(cudaStreamSynchronize(stream));
+    if (stats) *stats = d3g_predicate_stats{nq, int64_t(host_counters[1])};
+    const uint32_t bits = uint32_t(host_counters[0]);
+    if (bits & ST_INTERNAL) {
+        set_error("d3g_predicates_noalloc_device: point index out of range");
+        return D3G_ERR_INVALID_INPUT;
+    }
+    return status_from_bits(bits);
+}
+
 }  // namespace d3g
+
+extern "C" int d3g_predicates_noalloc_device(const double* d_pts, int64_t n_pts, const int32_t* d_idx,
+                                             int64_t n_queries, int kind, int8_t* d_sign_out,
+                                             void* stream, d3g_predicate_stats* stats) {
+    return d3g::predicates_noalloc_device(d_pts, n_pts, d_idx, n_queries, kind, d_sign_out,
+                                          static_cast<cudaStream_t>(stream), stats);
+}

@@ -93,6 +93,24 @@ int d3g_predicates_device(const double* d_pts, int64_t n_pts, const int32_t* d_i
                           int64_t n_queries, int kind, int8_t* d_sign_out, void* stream,
                           d3g_predicate_stats* stats);
 
+/* The same as d3g_predicates_device, for callers that cannot allocate device
+ * memory (a framework whose caching allocator has reserved the device, or a path
+ * where an allocation's implicit synchronisation or failure is unacceptable).
+ * No counterpart in the reference, which has no device code.
+ *   - Allocates nothing: the exact-stage queue and counters live in a fixed
+ *     array of this library (8 MiB per device that loads it, held until exit).
+ *   - At most D3G_NOALLOC_MAX_QUERIES queries per call; more returns
+ *     D3G_ERR_INVALID_ARGUMENT without touching the device.
+ *   - The first call on a device looks up the array's device address; make that
+ *     first call before any stream capture.
+ *   - Every call reuses the same array (the counters are cleared per call):
+ *     calls that overlap on the GPU, on any streams, race with each other.
+ * Synchronises `stream`. */
+#define D3G_NOALLOC_MAX_QUERIES (1 << 20)
+int d3g_predicates_noalloc_device(const double* d_pts, int64_t n_pts, const int32_t* d_idx,
+                                  int64_t n_queries, int kind, int8_t* d_sign_out, void* stream,
+                                  d3g_predicate_stats* stats);
+
 /* del3d::orient2d(px,py,qx,qy,rx,ry) over `six` (6 doubles per query); host pointers. */
 int d3g_orient2d(const double* six, int64_t n_queries, int8_t* sign_out);
 

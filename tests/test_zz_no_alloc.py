@@ -1,0 +1,89 @@
+"""d3g_predicates_noalloc_device: the predicate entry point for callers that
+cannot allocate device memory (its scratch is a fixed array of the library).
+
+Its signs must equal those of the allocating entry point d3g_predicates_device
+exactly (signs are exact: the tolerance is zero), on two calls in a row - the
+second call reuses the array the first one left behind.  Collected last so a
+run that stops at the first failure has run everything else already.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import del3d_b200 as d3
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+MAX_QUERIES = 1 << 20
+
+
+def _lib():
+    lib = d3.library()
+    fn = lib.d3g_predicates_noalloc_device
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    return lib
+
+
+def _run(fn, pts, idx, kind, torch):
+    out = torch.zeros(idx.shape[0], dtype=torch.int8, device=pts.device)
+    st = fn(pts.data_ptr(), pts.shape[0], idx.data_ptr(), idx.shape[0], kind, out.data_ptr(), None,
+            None)
+    assert st == 0, d3.library().d3g_last_error().decode()
+    return out.cpu().numpy()
+
+
+def _inputs(torch, dev, seed):
+    # Quantised surface samples (many exact ties: the exact-stage queue is used)
+    # mixed with generic points.
+    rng = np.random.default_rng(seed)
+    pts = np.concatenate([oracle.ps_sphere(400, 8, seed), oracle.ps_box_shell(6),
+                          rng.uniform(-1, 1, (3000, 3))])
+    idx = rng.integers(0, len(pts), (200000, 5)).astype(np.int32)
+    return (torch.from_numpy(pts).to(dev), torch.from_numpy(np.ascontiguousarray(idx)).to(dev))
+
+
+@pytest.mark.parametrize("kind", [d3.ORIENT3D, d3.IN_SPHERE, d3.IN_SPHERE_UNPERTURBED,
+                                  d3.COPLANAR_IN_CIRCLE])
+def test_noalloc_matches_allocating_entry_point(cuda, kind):
+    import torch
+
+    lib = _lib()
+    k = lib.d3g_predicate_arity(kind)
+    for call, seed in enumerate((1, 2)):          # two calls in a row
+        pts, idx5 = _inputs(torch, cuda, seed)
+        idx = idx5[:, :k].contiguous()
+        got = _run(lib.d3g_predicates_noalloc_device, pts, idx, kind, torch)
+        want = _run(lib.d3g_predicates_device, pts, idx, kind, torch)
+        assert (got == want).all(), f"call {call}: signs differ from d3g_predicates_device"
+
+
+def test_noalloc_exact_stage_used_and_counted(cuda):
+    import torch
+
+    lib = _lib()
+    pts, idx = _inputs(torch, cuda, 3)
+    st = (ctypes.c_int64 * 2)()
+    out = torch.zeros(idx.shape[0], dtype=torch.int8, device=cuda)
+    assert lib.d3g_predicates_noalloc_device(pts.data_ptr(), pts.shape[0], idx.data_ptr(),
+                                             idx.shape[0], d3.IN_SPHERE, out.data_ptr(), None,
+                                             ctypes.cast(st, ctypes.c_void_p)) == 0
+    assert st[0] == idx.shape[0] and st[1] > 0     # some queries reached the exact stage
+    ref = oracle.ref_predicate("in_sphere", pts.cpu().numpy(), idx.cpu().numpy())
+    assert (out.cpu().numpy() == ref).all()
+
+
+def test_noalloc_rejects_too_many_queries(cuda):
+    import torch
+
+    lib = _lib()
+    pts = torch.zeros((8, 3), dtype=torch.float64, device=cuda)
+    idx = torch.zeros((4, 5), dtype=torch.int32, device=cuda)
+    out = torch.zeros(4, dtype=torch.int8, device=cuda)
+    st = lib.d3g_predicates_noalloc_device(pts.data_ptr(), 8, idx.data_ptr(), MAX_QUERIES + 1,
+                                           d3.IN_SPHERE, out.data_ptr(), None, None)
+    assert st == 1   # D3G_ERR_INVALID_ARGUMENT, before any device work
+    assert b"D3G_NOALLOC_MAX_QUERIES" in lib.d3g_last_error()
