@@ -16,8 +16,11 @@
 //        decreases, so a thread per position resolves it.
 // 2. Multiscale split into levels [floor(n/8^(k+1)), floor(n/8^k)) while a
 //    range holds at least 64 points (spatial_sort.cpp:130-137).
-// 3. Within each level the points are ordered along a space-filling curve.
+// 3. Each level is ordered by the reference's Hilbert median splits, bit for bit
+//    (see k_select / k_small_sort below).
 #include "device_util.cuh"
+
+#include <vector>
 
 namespace d3g {
 namespace {
@@ -149,57 +152,198 @@ __global__ void k_final(const int32_t* __restrict__ j, const int32_t* __restrict
     }
 }
 
-// ---- placeholder in-level curve order: Morton keys inside BRIO levels ---------
+// ---- the Hilbert median splits (spatial_sort.cpp:40-117) -------------------------
+//
+// Every split position is begin + (end - begin) / 2 whatever the data, so the
+// host knows the whole recursion tree in advance and only the permutations need
+// the device.  Ranges of more than kSmall points are split by k_select, one
+// block per quickselect task; smaller ranges finish their whole recursion in
+// shared memory (k_small_sort).
 
-__global__ void k_bbox(const double* __restrict__ xyz, int64_t n, unsigned long long* bb) {
-    unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0};
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += int64_t(gridDim.x) * blockDim.x)
-        for (int a = 0; a < 3; ++a) {
-            const unsigned long long k = dbl_order_key(xyz[3 * i + a]);
-            lo[a] = k < lo[a] ? k : lo[a];
-            hi[a] = k > hi[a] ? k : hi[a];
+constexpr int kSelThreads = 512;
+constexpr int kSmall = 1024;
+
+/// The points being ordered: index plus coordinates, structure of arrays.
+struct Elems {
+    int32_t* idx;
+    double* x;
+    double* y;
+    double* z;
+};
+
+__device__ __forceinline__ double coord(const Elems& E, int axis, int j) {
+    return axis == 0 ? E.x[j] : (axis == 1 ? E.y[j] : E.z[j]);
+}
+
+__device__ __forceinline__ void move(const Elems& from, int i, const Elems& to, int j) {
+    to.idx[j] = from.idx[i];
+    to.x[j] = from.x[i];
+    to.y[j] = from.y[i];
+    to.z[j] = from.z[i];
+}
+
+/// The reference's Cmp (spatial_sort.cpp:25-36) called as cmp(element, pivot).
+__device__ __forceinline__ bool before_pivot(double c, double p, int up) {
+    return up ? (p < c) : (c < p);
+}
+
+struct SelTask {
+    int left, end, nth, axis, up;   // nth_element_deterministic on [left, end)
+};
+
+/// One block per task: the reference's middle-pivot quickselect
+/// (spatial_sort.cpp:60-71), each Lomuto partition (:40-51) done in parallel.
+/// A Lomuto pass moves the elements that compare before the pivot to the front
+/// in their original order; the others end up rotated: the element that lands
+/// on a "not before" slot q is the one scanned at q if that one was not before
+/// the pivot, and otherwise - the before-element at q having been swapped out to
+/// its rank position - whatever landed there, recursively.  Those chains are
+/// disjoint and strictly decreasing, and each thread follows its own.
+__global__ void __launch_bounds__(kSelThreads) k_select(const SelTask* __restrict__ tasks, Elems E,
+                                                         Elems B, int32_t* __restrict__ rk) {
+    typedef cub::BlockScan<int, kSelThreads> BlockScan;
+    __shared__ typename BlockScan::TempStorage scan_tmp;
+    const SelTask t = tasks[blockIdx.x];
+    if (t.end - t.left < 2) return;
+    int left = t.left, right = t.end - 1;
+    for (;;) {
+        const int pm = left + (right - left) / 2;
+        __syncthreads();
+        if (threadIdx.x == 0 && pm != right) {
+            move(E, pm, B, right);          // B as a one-element temporary
+            move(E, right, E, pm);
+            move(B, right, E, right);
         }
-    for (int a = 0; a < 3; ++a) {
-        atomicMin(bb + a, lo[a]);
-        atomicMax(bb + 3 + a, hi[a]);
+        __syncthreads();
+        const double P = coord(E, t.axis, right);
+        int running = 0;
+        for (int base = left; base < right; base += kSelThreads) {
+            const int j = base + int(threadIdx.x);
+            int less = 0;
+            if (j < right) less = before_pivot(coord(E, t.axis, j), P, t.up) ? 1 : 0;
+            int excl = 0, total = 0;
+            BlockScan(scan_tmp).ExclusiveSum(less, excl, total);
+            __syncthreads();
+            if (j < right) {
+                rk[j] = less ? running + excl : -1;
+                if (less) move(E, j, B, left + running + excl);
+            }
+            running += total;
+        }
+        const int L = running;
+        __syncthreads();
+        for (int q = left + L + int(threadIdx.x); q < right; q += kSelThreads) {
+            int x = q;
+            while (rk[x] >= 0) x = left + rk[x];
+            move(E, x, B, q == left + L ? right : q);
+        }
+        if (threadIdx.x == 0) move(E, right, B, left + L);
+        __syncthreads();
+        for (int j = left + int(threadIdx.x); j <= right; j += kSelThreads) move(B, j, E, j);
+        const int np = left + L;
+        if (np == t.nth) break;
+        if (t.nth < np) right = np - 1;
+        else left = np + 1;
     }
 }
 
-__device__ __forceinline__ uint64_t spread3(uint64_t x) {   // 16 bits -> every third bit
-    x &= 0xFFFF;
-    x = (x | (x << 32)) & 0x0000FFFF0000FFFFull;
-    x = (x | (x << 16)) & 0x00FF0000FF0000FFull;
-    x = (x | (x << 8)) & 0xF00F00F00F00F00Full;
-    x = (x | (x << 4)) & 0x30C30C30C30C30C3ull;
-    x = (x | (x << 2)) & 0x9249249249249249ull;
-    return x;
+struct Seg {
+    int begin, end, x, ux, uy, uz;   // recursive_sort(begin, end, x, upx, upy, upz)
+};
+
+struct Local {
+    int32_t* idx;
+    double* c[3];
+};
+
+__device__ void local_swap(Local& L, int i, int j) {
+    const int32_t ti = L.idx[i];
+    L.idx[i] = L.idx[j];
+    L.idx[j] = ti;
+    for (int a = 0; a < 3; ++a) {
+        const double tc = L.c[a][i];
+        L.c[a][i] = L.c[a][j];
+        L.c[a][j] = tc;
+    }
 }
 
-__global__ void k_level_morton(const double* __restrict__ xyz, const int32_t* __restrict__ order,
-                               int64_t n, const unsigned long long* bb, const int64_t* bounds,
-                               int nlev, uint64_t* __restrict__ keys) {
-    double lo[3], ext[3];
-    for (int a = 0; a < 3; ++a) {
-        lo[a] = dbl_from_order_key(bb[a]);
-        const double hi = dbl_from_order_key(bb[3 + a]);
-        ext[a] = hi > lo[a] ? hi - lo[a] : 1.0;
+/// spatial_sort.cpp:40-79, verbatim in shared memory; [left, end).
+__device__ int local_split(Local& L, int begin, int end, int axis, int up) {
+    if (begin >= end) return begin;
+    const int middle = begin + (end - begin) / 2;
+    int left = begin, right = end - 1;
+    if (left == right) return middle;
+    for (;;) {
+        const int pm = left + (right - left) / 2;
+        local_swap(L, pm, right);
+        const double P = L.c[axis][right];
+        int result = left;
+        for (int it = left; it != right; ++it) {
+            if (before_pivot(L.c[axis][it], P, up)) {
+                local_swap(L, result, it);
+                ++result;
+            }
+        }
+        local_swap(L, right, result);
+        if (result == middle) return middle;
+        if (middle < result) right = result - 1;
+        else left = result + 1;
     }
+}
+
+/// One warp per range of at most kSmall points: the whole remaining recursion
+/// (spatial_sort.cpp:95-117) by lane 0 in shared memory.
+__global__ void __launch_bounds__(32) k_small_sort(const Seg* __restrict__ segs, Elems E) {
+    __shared__ int32_t sidx[kSmall];
+    __shared__ double sc[3][kSmall];
+    const Seg g = segs[blockIdx.x];
+    const int m = g.end - g.begin;
+    for (int j = threadIdx.x; j < m; j += 32) {
+        sidx[j] = E.idx[g.begin + j];
+        sc[0][j] = E.x[g.begin + j];
+        sc[1][j] = E.y[g.begin + j];
+        sc[2][j] = E.z[g.begin + j];
+    }
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        Local L{sidx, {sc[0], sc[1], sc[2]}};
+        Seg stack[64];
+        int top = 0;
+        stack[top++] = Seg{0, m, g.x, g.ux, g.uy, g.uz};
+        while (top > 0) {
+            const Seg f = stack[--top];
+            if (f.end - f.begin <= 8) continue;
+            const int x = f.x, y = (x + 1) % 3, z = (x + 2) % 3;
+            const int m0 = f.begin, m8 = f.end;
+            const int m4 = local_split(L, m0, m8, x, f.ux);
+            const int m2 = local_split(L, m0, m4, y, f.uy);
+            const int m1 = local_split(L, m0, m2, z, f.uz);
+            const int m3 = local_split(L, m2, m4, z, !f.uz);
+            const int m6 = local_split(L, m4, m8, y, !f.uy);
+            const int m5 = local_split(L, m4, m6, z, f.uz);
+            const int m7 = local_split(L, m6, m8, z, !f.uz);
+            stack[top++] = Seg{m0, m1, z, f.uz, f.ux, f.uy};
+            stack[top++] = Seg{m1, m2, y, f.uy, f.uz, f.ux};
+            stack[top++] = Seg{m2, m3, y, f.uy, f.uz, f.ux};
+            stack[top++] = Seg{m3, m4, x, f.ux, !f.uy, !f.uz};
+            stack[top++] = Seg{m4, m5, x, f.ux, !f.uy, !f.uz};
+            stack[top++] = Seg{m5, m6, y, !f.uy, f.uz, !f.ux};
+            stack[top++] = Seg{m6, m7, y, !f.uy, f.uz, !f.ux};
+            stack[top++] = Seg{m7, m8, z, !f.uz, !f.ux, f.uy};
+        }
+    }
+    __syncwarp();
+    for (int j = threadIdx.x; j < m; j += 32) E.idx[g.begin + j] = sidx[j];
+}
+
+__global__ void k_gather_xyz(const double* __restrict__ xyz, const int32_t* __restrict__ order, int64_t n,
+                             double* __restrict__ x, double* __restrict__ y, double* __restrict__ z) {
     for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n;
          p += int64_t(gridDim.x) * blockDim.x) {
-        // Level: bounds[0] = n > bounds[1] > ... ; position p is in level k if
-        // bounds[k+1] <= p < bounds[k]; the coarsest (highest k) goes first.
-        int lvl = 0;
-        while (lvl + 1 < nlev && p < bounds[lvl + 1]) ++lvl;
         const int64_t i = order[p];
-        uint64_t m = 0;
-        for (int a = 0; a < 3; ++a) {
-            double u = (xyz[3 * i + a] - lo[a]) / ext[a];
-            u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
-            const uint64_t c = uint64_t(u * 65535.0);
-            m |= spread3(c) << a;
-        }
-        keys[p] = (uint64_t(nlev - 1 - lvl) << 48) | m;
+        x[p] = xyz[3 * i];
+        y[p] = xyz[3 * i + 1];
+        z[p] = xyz[3 * i + 2];
     }
 }
 
@@ -300,29 +444,98 @@ int multiscale_bounds(int64_t n, int64_t* b, int cap) {
     return k;   // levels: [b[k+1], b[k]) for k < count-1, plus [0, b[count-1])
 }
 
+namespace {
+
+template <class T>
+int upload(const std::vector<T>& v, DevBuf<T>& d, cudaStream_t s) {
+    D3G_TRY(d.alloc(v.size(), s));
+    if (!v.empty())
+        D3G_CUDA(cudaMemcpyAsync(d.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+    return D3G_OK;
+}
+
+}  // namespace
+
 int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaStream_t s) {
     if (n <= 0) return D3G_OK;
     D3G_TRY(shuffle_device(n, d_order, s));
     if (n < 2) return D3G_OK;
+    DevBuf<double> ex, ey, ez, bx, by, bz;
+    DevBuf<int32_t> bidx, rk;
+    D3G_TRY(ex.alloc(size_t(n), s));
+    D3G_TRY(ey.alloc(size_t(n), s));
+    D3G_TRY(ez.alloc(size_t(n), s));
+    k_gather_xyz<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, d_order, n, ex.p, ey.p, ez.p);
+    const Elems E{d_order, ex.p, ey.p, ez.p};
+
+    // Roots: the multiscale levels (spatial_sort.cpp:130-137), each Hilbert-sorted
+    // from axis x with every direction "down".
     int64_t hb[64];
     const int nb = multiscale_bounds(n, hb, 63);
-    DevBuf<int64_t> bounds;
-    DevBuf<unsigned long long> bb;
-    DevBuf<uint64_t> keys, keys2;
-    DevBuf<int32_t> tmp;
-    D3G_TRY(bounds.alloc(size_t(nb), s));
-    D3G_TRY(bb.alloc(6, s));
-    D3G_CUDA(cudaMemcpyAsync(bounds.p, hb, sizeof(int64_t) * nb, cudaMemcpyHostToDevice, s));
-    const unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0, 0, 0};
-    D3G_CUDA(cudaMemcpyAsync(bb.p, init, sizeof init, cudaMemcpyHostToDevice, s));
-    k_bbox<<<grid_for(n, 256, kNumSMs * 4), 256, 0, s>>>(d_xyz, n, bb.p);
-    D3G_TRY(keys.alloc(size_t(n), s));
-    D3G_TRY(keys2.alloc(size_t(n), s));
-    D3G_TRY(tmp.alloc(size_t(n), s));
-    k_level_morton<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, d_order, n, bb.p, bounds.p, nb, keys.p);
-    D3G_TRY(sort_pairs(keys.p, keys2.p, d_order, tmp.p, n, 0, 48 + bits_for(uint64_t(nb)), s));
-    D3G_CUDA(cudaMemcpyAsync(d_order, tmp.p, sizeof(int32_t) * size_t(n), cudaMemcpyDeviceToDevice, s));
-    D3G_CUDA(cudaGetLastError());
+    std::vector<Seg> big, small;
+    auto classify = [&](const Seg& g) {
+        const int len = g.end - g.begin;
+        if (len <= 8) return;
+        if (len <= kSmall) small.push_back(g);
+        else big.push_back(g);
+    };
+    for (int k = 0; k < nb; ++k) {
+        const int lo = int(k + 1 < nb ? hb[k + 1] : 0);
+        classify(Seg{lo, int(hb[k]), 0, 0, 0, 0});
+    }
+    if (!big.empty()) {
+        D3G_TRY(bidx.alloc(size_t(n), s));
+        D3G_TRY(bx.alloc(size_t(n), s));
+        D3G_TRY(by.alloc(size_t(n), s));
+        D3G_TRY(bz.alloc(size_t(n), s));
+        D3G_TRY(rk.alloc(size_t(n), s));
+    }
+    const Elems B{bidx.p, bx.p, by.p, bz.p};
+    auto mid = [](int b, int e) { return b + (e - b) / 2; };
+    while (!big.empty()) {
+        std::vector<SelTask> ta, tb, tc;
+        std::vector<Seg> next;
+        auto task = [](std::vector<SelTask>& v, int b, int e, int axis, int up) {
+            if (e - b >= 2) v.push_back(SelTask{b, e, b + (e - b) / 2, axis, up});
+        };
+        for (const Seg& g : big) {
+            const int x = g.x, y = (x + 1) % 3, z = (x + 2) % 3;
+            const int m0 = g.begin, m8 = g.end, m4 = mid(m0, m8);
+            const int m2 = mid(m0, m4), m6 = mid(m4, m8);
+            const int m1 = mid(m0, m2), m3 = mid(m2, m4), m5 = mid(m4, m6), m7 = mid(m6, m8);
+            task(ta, m0, m8, x, g.ux);
+            task(tb, m0, m4, y, g.uy);
+            task(tb, m4, m8, y, !g.uy);
+            task(tc, m0, m2, z, g.uz);
+            task(tc, m2, m4, z, !g.uz);
+            task(tc, m4, m6, z, g.uz);
+            task(tc, m6, m8, z, !g.uz);
+            const Seg kids[8] = {{m0, m1, z, g.uz, g.ux, g.uy},   {m1, m2, y, g.uy, g.uz, g.ux},
+                                 {m2, m3, y, g.uy, g.uz, g.ux},   {m3, m4, x, g.ux, !g.uy, !g.uz},
+                                 {m4, m5, x, g.ux, !g.uy, !g.uz}, {m5, m6, y, !g.uy, g.uz, !g.ux},
+                                 {m6, m7, y, !g.uy, g.uz, !g.ux}, {m7, m8, z, !g.uz, !g.ux, g.uy}};
+            for (const Seg& k : kids) {
+                const int len = k.end - k.begin;
+                if (len <= 8) continue;
+                if (len <= kSmall) small.push_back(k);
+                else next.push_back(k);
+            }
+        }
+        for (const std::vector<SelTask>* phase : {&ta, &tb, &tc}) {
+            if (phase->empty()) continue;
+            DevBuf<SelTask> dt;
+            D3G_TRY(upload(*phase, dt, s));
+            k_select<<<unsigned(phase->size()), kSelThreads, 0, s>>>(dt.p, E, B, rk.p);
+            D3G_CUDA(cudaGetLastError());
+        }
+        big.swap(next);
+    }
+    if (!small.empty()) {
+        DevBuf<Seg> ds;
+        D3G_TRY(upload(small, ds, s));
+        k_small_sort<<<unsigned(small.size()), 32, 0, s>>>(ds.p, E);
+        D3G_CUDA(cudaGetLastError());
+    }
     return D3G_OK;
 }
 

@@ -24,6 +24,12 @@ CASES = {
     "uniform20k": lambda: d3.gen_uniform(20000, 1),
     "sphere_q1024": lambda: d3.gen_sphere(20000, 5),
     "clusters": lambda: d3.gen_clusters(20000, 7),
+    # Duplicates: a repeated point keeps the index of its copy that comes last in
+    # the reference's spatial order (src/triangulation.cpp:77-81).
+    "dup_grid": lambda: np.random.default_rng(3).integers(0, 6, (3000, 3)).astype(np.float64),
+    "dup_copies": lambda: np.concatenate([d3.gen_uniform(5000, 2), d3.gen_uniform(5000, 2)[::3],
+                                          -np.zeros((7, 3)), np.zeros((5, 3))]),
+    "sphere_q_dups": lambda: d3.gen_sphere(30000, 5, q=64, dedupe=False),
 }
 
 
