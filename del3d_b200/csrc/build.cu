@@ -48,8 +48,12 @@ constexpr int kInf = -1;
 constexpr int kWalkLimit = 1 << 20;
 constexpr int kRotateLimit = 1 << 16;
 constexpr int kRoundsPerBatch = 16;
+// Scratch of a worker in a normal round, and of each of the kBigSlots workers
+// served at a time in a big round.
+constexpr int kCavCap = 256, kFacCap = 512;
+constexpr int kBigSlots = 64, kBigCav = 16384, kBigFac = 32768;
 
-enum : int { WS_DONE = 0, WS_CAND = 1, WS_LOST = 2, WS_WIN = 3, WS_OVERFLOW = 4, WS_FAIL = 5 };
+enum : int { WS_DONE = 0, WS_CAND = 1, WS_LOST = 2, WS_WIN = 3, WS_PARKED = 4, WS_FAIL = 5 };
 
 __device__ __forceinline__ Pt vpt(const double* __restrict__ vx, int v) {
     const double* p = vx + 3 * int64_t(v);
@@ -84,6 +88,8 @@ struct Tables {
 };
 
 struct Workers {
+    const int* list;  // big mode: the workers served (warp i serves list[i]); null otherwise
+    int* parked;  // 1 while the worker's point needs the big scratch
     int* cur;     // current point (vertex id) of each worker
     int* beg;     // start of its chunk
     int* end;     // end of its chunk
@@ -106,10 +112,10 @@ struct Workers {
 struct Round {
     const unsigned* round;    // current round number (device), set by k_round_begin
     int skip[4];              // the initial tet's vertices (already inserted)
-    int* counters;            // [0] active workers, [1] overflowed workers, [2] winners
+    int* counters;            // [0] active workers, [1] parked workers, [2] winners
     unsigned long long* sums; // [0] region tets, [1] boundary facets of the winners
     unsigned long long* totals; // [0] winners, [1] attempts, [2] rounds with work,
-                                // [3] overflow seen, [4] stalled round seen, [5] active
+                                // [3] parked workers, [4] stalled round seen, [5] active
     uint32_t* status;
 };
 
@@ -129,12 +135,12 @@ __global__ void k_round_begin(Round R) {
 /// Folds one round's counters into the running totals; flags a round in which
 /// workers were active but nobody won (the earliest pending point must win).
 __global__ void k_round_end(Round R) {
-    const int active = R.counters[0], over = R.counters[1], won = R.counters[2];
+    const int active = R.counters[0], parked = R.counters[1], won = R.counters[2];
     R.totals[0] += (unsigned long long)won;
     R.totals[1] += (unsigned long long)(active + won);
     if (active + won > 0) R.totals[2] += 1;
-    if (over > 0) R.totals[3] = 1;
-    if (active > 0 && won == 0 && over == 0) R.totals[4] = 1;
+    R.totals[3] = (unsigned long long)parked;
+    if (active > 0 && won == 0) R.totals[4] = 1;
     R.totals[5] = (unsigned long long)active;
 }
 
@@ -237,11 +243,13 @@ __device__ int next_point(const Workers& W, int w, const int* skip) {
 __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R, const double* __restrict__ vx,
                                                 int first) {
     const int lane = threadIdx.x & 31;
-    const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (w >= W.n) return;
+    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (slot >= W.n) return;
+    const int w = W.list ? W.list[slot] : slot;
     const int v = W.cur[w];
-    if (v < 0) {
-        if (lane == 0) W.state[w] = WS_DONE;
+    // Normal rounds leave parked workers alone; big rounds serve only those.
+    if (v < 0 || (W.parked[w] != 0) != (W.list != nullptr)) {
+        if (lane == 0) W.state[w] = v < 0 ? WS_DONE : WS_PARKED;
         return;
     }
     const Pt p = vpt(vx, v);
@@ -253,8 +261,8 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
     }
     const unsigned long long key = claim_key(R, v);
     const unsigned long long mine = key >> 1;
-    int* cav = W.cav + int64_t(w) * W.cav_cap;
-    int* fac = W.fac + int64_t(w) * W.fac_cap;
+    int* cav = W.cav + int64_t(slot) * W.cav_cap;
+    int* fac = W.fac + int64_t(slot) * W.fac_cap;
     int lost = 0;
     if (lane == 0) {
         const unsigned long long old = atomicMin(T.claim + seed, key);
@@ -313,8 +321,11 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
         const unsigned mf = __ballot_sync(kFull, kind == 1);
         if (ncav + __popc(mc) > W.cav_cap || nfac + __popc(mf) > W.fac_cap) {
             if (lane == 0) {
-                W.state[w] = WS_OVERFLOW;
-                atomicAdd(R.counters + 1, 1);
+                // Too big for this scratch: park the worker until a big round
+                // (or, in a big round, report that even that was not enough).
+                W.state[w] = WS_PARKED;
+                if (W.list) report(R.status, ST_CAVITY_CAPACITY);
+                else W.parked[w] = 1;
             }
             return;
         }
@@ -335,12 +346,14 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
 /// One warp per candidate: it wins if it still holds every claim it made.
 __global__ void __launch_bounds__(128, 8) k_check(Tables T, Workers W, Round R, int first) {
     const int lane = threadIdx.x & 31;
-    const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (w >= W.n || W.state[w] != WS_CAND) return;
+    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (slot >= W.n) return;
+    const int w = W.list ? W.list[slot] : slot;
+    if (W.state[w] != WS_CAND) return;
     const int v = W.cur[w];
     const unsigned long long key = claim_key(R, v);
-    const int* cav = W.cav + int64_t(w) * W.cav_cap;
-    const int* fac = W.fac + int64_t(w) * W.fac_cap;
+    const int* cav = W.cav + int64_t(slot) * W.cav_cap;
+    const int* fac = W.fac + int64_t(slot) * W.fac_cap;
     const int ncav = W.ncav[w], nfac = W.nfac[w];
     bool ok = true;
     for (int k = lane; k < ncav; k += 32) ok = ok && T.claim[cav[k]] == key;
@@ -354,21 +367,22 @@ __global__ void __launch_bounds__(128, 8) k_check(Tables T, Workers W, Round R, 
 
 /// One warp per winner: re-star its region, one boundary facet per lane.
 __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R, int first) {
-    __shared__ int sh_count[2];
+    __shared__ int sh_count[3];
     const int lane = threadIdx.x & 31;
-    const int w = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (threadIdx.x < 2) sh_count[threadIdx.x] = 0;
+    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (threadIdx.x < 3) sh_count[threadIdx.x] = 0;
     __syncthreads();
-    const bool exists = w < W.n;
+    const bool exists = slot < W.n;
+    const int w = exists ? (W.list ? W.list[slot] : slot) : 0;
     const int state = exists ? W.state[w] : WS_DONE;
     const int v = exists ? W.cur[w] : -1;
     bool advanced = false;
     if (state == WS_WIN) {
         const unsigned long long key = claim_key(R, v);
-        const int* cav = W.cav + int64_t(w) * W.cav_cap;
-        const int* fac = W.fac + int64_t(w) * W.fac_cap;
-        int4* sv = W.st_v + int64_t(w) * W.fac_cap;
-        int4* sn = W.st_n + int64_t(w) * W.fac_cap;
+        const int* cav = W.cav + int64_t(slot) * W.cav_cap;
+        const int* fac = W.fac + int64_t(slot) * W.fac_cap;
+        int4* sv = W.st_v + int64_t(slot) * W.fac_cap;
+        int4* sn = W.st_n + int64_t(slot) * W.fac_cap;
         const int C = W.ncav[w], F = W.nfac[w];
         const int extra = F > C ? F - C : 0;
         int base = 0, ok = 1;
@@ -463,16 +477,26 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
         int cur = v;
         if (advanced) {
             W.last[w] = v;
+            W.parked[w] = 0;
             cur = next_point(W, w, R.skip);
         }
-        if (state != WS_DONE && cur >= 0) atomicAdd(sh_count, 1);
-        if (advanced) atomicAdd(sh_count + 1, 1);
+        if (cur >= 0 && W.parked[w]) atomicAdd(sh_count + 1, 1);     // waits for a big round
+        else if (state != WS_DONE && cur >= 0) atomicAdd(sh_count, 1);
+        if (advanced) atomicAdd(sh_count + 2, 1);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         if (sh_count[0]) atomicAdd(R.counters, sh_count[0]);
-        if (sh_count[1]) atomicAdd(R.counters + 2, sh_count[1]);
+        if (sh_count[1]) atomicAdd(R.counters + 1, sh_count[1]);
+        if (sh_count[2]) atomicAdd(R.counters + 2, sh_count[2]);
     }
+}
+
+/// Lists the parked workers (for the big rounds).
+__global__ void k_collect_parked(Workers W, int* list, int* count) {
+    const int w = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (w >= W.n) return;
+    if (W.parked[w] && W.cur[w] >= 0) list[atomicAdd(count, 1)] = w;
 }
 
 /// Workers of one level [lb, le): one chunk each.  Each starts at a scattered
@@ -489,6 +513,7 @@ __global__ void k_setup_level(Workers W, int lb, int le, int chunk, int plb, int
     W.beg[w] = b;
     W.end[w] = e;
     W.off[w] = off;
+    W.parked[w] = 0;
     W.done[w] = 0;
     W.last[w] = -1;
     const int skip[4] = {skip4.x, skip4.y, skip4.z, skip4.w};
@@ -973,14 +998,17 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         maxw = std::max<int64_t>(maxw, (cnt + ch - 1) / ch);
     }
     Workers W;
-    W.cav_cap = 256;
-    W.fac_cap = 512;
+    W.cav_cap = kCavCap;
+    W.fac_cap = kFacCap;
     W.n = maxw;
     DevBuf<int> wcur, wbeg, wend, woff, wdone, wlast, wguide, wstate, wncav, wnfac, wcav, wfac, counters;
+    DevBuf<int> wparked, blist, bcount, bcav, bfac;
+    DevBuf<int4> bsv, bsn;
     DevBuf<int4> wsv, wsn;
     D3G_TRY(wcur.alloc(size_t(maxw), s));
     D3G_TRY(wend.alloc(size_t(maxw), s));
     D3G_TRY(wbeg.alloc(size_t(maxw), s));
+    D3G_TRY(wparked.alloc(size_t(maxw), s));
     D3G_TRY(woff.alloc(size_t(maxw), s));
     D3G_TRY(wdone.alloc(size_t(maxw), s));
     D3G_TRY(wlast.alloc(size_t(maxw), s));
@@ -1004,6 +1032,8 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     W.cur = wcur.p;
     W.end = wend.p;
     W.beg = wbeg.p;
+    W.list = nullptr;
+    W.parked = wparked.p;
     W.off = woff.p;
     W.done = wdone.p;
     W.last = wlast.p;
@@ -1039,6 +1069,67 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
                 if (e[i]) cudaEventDestroy(e[i]);
         }
     } ev_guard{kev};
+    // Big rounds: workers whose conflict region outgrew the normal scratch.
+    Workers WB = W;
+    WB.cav_cap = kBigCav;
+    WB.fac_cap = kBigFac;
+    auto big_rounds = [&]() -> int {
+        if (!blist.p) {
+            D3G_TRY(blist.alloc(size_t(maxw), s));
+            D3G_TRY(bcount.alloc(1, s));
+            D3G_TRY(bcav.alloc(size_t(kBigSlots) * kBigCav, s));
+            D3G_TRY(bfac.alloc(size_t(kBigSlots) * kBigFac, s));
+            D3G_TRY(bsv.alloc(size_t(kBigSlots) * kBigFac, s));
+            D3G_TRY(bsn.alloc(size_t(kBigSlots) * kBigFac, s));
+        }
+        for (;;) {
+            D3G_CUDA(cudaMemsetAsync(bcount.p, 0, sizeof(int), s));
+            k_collect_parked<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, blist.p, bcount.p);
+            int nparked = 0;
+            D3G_CUDA(cudaMemcpyAsync(&nparked, bcount.p, sizeof nparked, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaStreamSynchronize(s));
+            if (nparked == 0) return D3G_OK;
+            WB = W;
+            WB.list = blist.p;
+            WB.n = std::min(nparked, kBigSlots);
+            WB.cav = bcav.p;
+            WB.fac = bfac.p;
+            WB.st_v = bsv.p;
+            WB.st_n = bsn.p;
+            WB.cav_cap = kBigCav;
+            WB.fac_cap = kBigFac;
+            const unsigned gb = unsigned((int64_t(WB.n) * 32 + 127) / 128);
+            for (;;) {
+                if (++round > max_rounds) {
+                    set_error("d3g_build: insertion round limit reached");
+                    return D3G_ERR_ROUND_LIMIT;
+                }
+                unsigned long long before = 0;
+                D3G_CUDA(cudaMemcpyAsync(&before, totals.p, sizeof before, cudaMemcpyDeviceToHost, s));
+                k_round_begin<<<1, 1, 0, s>>>(Rd);
+                k_cavity<<<gb, 128, 0, s>>>(T, WB, Rd, vx.p, 0);
+                k_check<<<gb, 128, 0, s>>>(T, WB, Rd, 0);
+                k_restar<<<gb, 128, 0, s>>>(T, WB, Rd, 0);
+                k_round_end<<<1, 1, 0, s>>>(Rd);
+                unsigned long long ht[6];
+                uint32_t hs = 0;
+                D3G_CUDA(cudaMemcpyAsync(ht, totals.p, sizeof ht, cudaMemcpyDeviceToHost, s));
+                D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+                D3G_CUDA(cudaStreamSynchronize(s));
+                if (hs != 0) {
+                    const int st = status_from_bits(hs);
+                    if (st == D3G_ERR_CAVITY_CAPACITY)
+                        set_error("d3g_build: a conflict region exceeded the big-round scratch");
+                    return st;
+                }
+                if (ht[3] == 0) break;           // every listed worker got its point in
+                if (ht[0] == before) {           // the earliest parked point must win
+                    set_error("d3g_build: a big round made no progress");
+                    return D3G_ERR_INTERNAL;
+                }
+            }
+        }
+    };
     // Levels from the coarsest ([0, hb[nb-1])) to the finest ([hb[1], hb[0])).
     for (int k = nb - 1; k >= 0; --k) {
         const int lb = int(k + 1 < nb ? hb[k + 1] : 0);
@@ -1119,10 +1210,6 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
                 if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");
                 return st;
             }
-            if (ht[3]) {
-                set_error("d3g_build: a conflict region exceeded the per-worker scratch");
-                return D3G_ERR_CAVITY_CAPACITY;
-            }
             if (ht[4]) {
                 set_error("d3g_build: an insertion round made no progress");
                 return D3G_ERR_INTERNAL;
@@ -1139,7 +1226,11 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
             }
             won = (long long)ht[0] - won_before;
             attempts = (long long)ht[1] - att_before;
-            if (ht[5] == 0) break;
+            if (ht[5] != 0) continue;
+            if (ht[3] == 0) break;
+            // Only parked workers are left: serve them in big rounds, up to
+            // kBigSlots at a time, each until its point is in.
+            D3G_TRY(big_rounds());
         }
         if (trace) {
             cudaEventRecord(ev1, s);
