@@ -20,6 +20,7 @@
 //    (see k_select / k_small_sort below).
 #include "device_util.cuh"
 
+#include <algorithm>
 #include <vector>
 
 namespace d3g {
@@ -244,6 +245,193 @@ __global__ void __launch_bounds__(kSelThreads) k_select(const SelTask* __restric
         if (np == t.nth) break;
         if (t.nth < np) right = np - 1;
         else left = np + 1;
+    }
+}
+
+// ---- the same quickselect across the whole GPU, for tasks too big for a block ----
+//
+// While a phase has tasks longer than kBlockSelectMax, each Lomuto pass of every
+// such task is spread over tiles of kTile elements: count the elements before
+// the pivot per tile, scan the counts, scatter them stably, resolve the rotated
+// rest by the same chains as k_select, copy back, update the range.  Tasks that
+// have shrunk below the limit are finished by k_select.
+
+constexpr int kTile = 1024;
+constexpr int kTileThreads = 256;
+constexpr int kBlockSelectMax = 1 << 16;
+
+struct TaskState {
+    int left, right, nth, axis, up, done;
+    double pivot;
+    int tile0, ntiles, L;
+};
+
+__device__ __forceinline__ int task_of_tile(const TaskState* __restrict__ ts, int ntask, int tile) {
+    int lo = 0, hi = ntask - 1;
+    while (lo < hi) {   // last task whose first tile <= tile
+        const int mid = (lo + hi + 1) >> 1;
+        if (ts[mid].tile0 <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+/// One block: pivot swap of every active task, tile counts and first tiles.
+__global__ void __launch_bounds__(1024) k_plan(TaskState* ts, int ntask, Elems E, Elems B, int* total) {
+    typedef cub::BlockScan<int, 1024> BlockScan;
+    __shared__ typename BlockScan::TempStorage tmp;
+    int running = 0;
+    for (int base = 0; base < ntask; base += 1024) {
+        const int t = base + int(threadIdx.x);
+        int tiles = 0;
+        if (t < ntask && !ts[t].done) {
+            TaskState& k = ts[t];
+            const int pm = k.left + (k.right - k.left) / 2;
+            if (pm != k.right) {
+                move(E, pm, B, k.right);
+                move(E, k.right, E, pm);
+                move(B, k.right, E, k.right);
+            }
+            k.pivot = coord(E, k.axis, k.right);
+            tiles = (k.right - k.left + kTile - 1) / kTile;
+        }
+        int excl = 0, sum = 0;
+        BlockScan(tmp).ExclusiveSum(tiles, excl, sum);
+        __syncthreads();
+        if (t < ntask) {
+            ts[t].tile0 = running + excl;
+            ts[t].ntiles = tiles;
+        }
+        running += sum;
+    }
+    if (threadIdx.x == 0) *total = running;
+}
+
+__global__ void __launch_bounds__(kTileThreads) k_tile_count(const TaskState* __restrict__ ts, int ntask,
+                                                             Elems E, const int* total,
+                                                             int* __restrict__ tile_less) {
+    typedef cub::BlockReduce<int, kTileThreads> BlockReduce;
+    __shared__ typename BlockReduce::TempStorage tmp;
+    const int T = *total;
+    for (int tile = blockIdx.x; tile < T; tile += gridDim.x) {
+        const TaskState& k = ts[task_of_tile(ts, ntask, tile)];
+        const int b = k.left + (tile - k.tile0) * kTile;
+        const int e = min(b + kTile, k.right);
+        int c = 0;
+        for (int j = b + int(threadIdx.x); j < e; j += kTileThreads)
+            c += before_pivot(coord(E, k.axis, j), k.pivot, k.up) ? 1 : 0;
+        const int sum = BlockReduce(tmp).Sum(c);
+        if (threadIdx.x == 0) tile_less[tile] = sum;
+        __syncthreads();
+    }
+}
+
+/// One block: exclusive scan of the tile counts; each task's L.
+__global__ void __launch_bounds__(1024) k_tile_scan(TaskState* ts, int ntask, const int* total,
+                                                    int* tile_less) {
+    typedef cub::BlockScan<int, 1024> BlockScan;
+    __shared__ typename BlockScan::TempStorage tmp;
+    const int T = *total;
+    int running = 0;
+    for (int base = 0; base < T; base += 1024) {
+        const int i = base + int(threadIdx.x);
+        const int v = i < T ? tile_less[i] : 0;
+        int excl = 0, sum = 0;
+        BlockScan(tmp).ExclusiveSum(v, excl, sum);
+        __syncthreads();
+        if (i < T) tile_less[i] = running + excl;   // now: elements before the pivot ahead of the tile
+        running += sum;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < ntask; t += 1024) {
+        TaskState& k = ts[t];
+        if (k.done) continue;
+        const int first = k.tile0, last = k.tile0 + k.ntiles;    // tiles [first, last)
+        const int end_off = last < T ? tile_less[last] : running;
+        k.L = end_off - tile_less[first];
+    }
+}
+
+__global__ void __launch_bounds__(kTileThreads) k_tile_scatter(const TaskState* __restrict__ ts, int ntask,
+                                                               Elems E, Elems B, const int* total,
+                                                               const int* __restrict__ tile_off,
+                                                               int32_t* __restrict__ rk) {
+    typedef cub::BlockScan<int, kTileThreads> BlockScan;
+    __shared__ typename BlockScan::TempStorage tmp;
+    const int T = *total;
+    for (int tile = blockIdx.x; tile < T; tile += gridDim.x) {
+        const TaskState& k = ts[task_of_tile(ts, ntask, tile)];
+        const int b = k.left + (tile - k.tile0) * kTile;
+        const int e = min(b + kTile, k.right);
+        int running = tile_off[tile] - tile_off[k.tile0];
+        for (int base = b; base < e; base += kTileThreads) {
+            const int j = base + int(threadIdx.x);
+            int less = 0;
+            if (j < e) less = before_pivot(coord(E, k.axis, j), k.pivot, k.up) ? 1 : 0;
+            int excl = 0, sum = 0;
+            BlockScan(tmp).ExclusiveSum(less, excl, sum);
+            __syncthreads();
+            if (j < e) {
+                rk[j] = less ? running + excl : -1;
+                if (less) move(E, j, B, k.left + running + excl);
+            }
+            running += sum;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTileThreads) k_tile_place(const TaskState* __restrict__ ts, int ntask,
+                                                             Elems E, Elems B, const int* total,
+                                                             const int32_t* __restrict__ rk) {
+    const int T = *total;
+    for (int tile = blockIdx.x; tile < T; tile += gridDim.x) {
+        const TaskState& k = ts[task_of_tile(ts, ntask, tile)];
+        const int b = k.left + (tile - k.tile0) * kTile;
+        const int e = min(b + kTile, k.right);
+        const int first_ge = k.left + k.L;
+        for (int q = max(b, first_ge) + int(threadIdx.x); q < e; q += kTileThreads) {
+            int x = q;
+            while (rk[x] >= 0) x = k.left + rk[x];
+            move(E, x, B, q == first_ge ? k.right : q);
+        }
+    }
+}
+
+__global__ void k_tile_pivot(const TaskState* __restrict__ ts, int ntask, Elems E, Elems B) {
+    for (int t = int(blockIdx.x) * blockDim.x + threadIdx.x; t < ntask; t += gridDim.x * blockDim.x)
+        if (!ts[t].done) move(E, ts[t].right, B, ts[t].left + ts[t].L);
+}
+
+__global__ void __launch_bounds__(kTileThreads) k_tile_copy(const TaskState* __restrict__ ts, int ntask,
+                                                            Elems E, Elems B, const int* total) {
+    const int T = *total;
+    for (int tile = blockIdx.x; tile < T; tile += gridDim.x) {
+        const TaskState& k = ts[task_of_tile(ts, ntask, tile)];
+        const int b = k.left + (tile - k.tile0) * kTile;
+        const int e = min(b + kTile, k.right);
+        for (int j = b + int(threadIdx.x); j < e; j += kTileThreads) move(B, j, E, j);
+    }
+}
+
+/// Per task: the pivot slot, the new range; counts the tasks still too big.
+__global__ void k_tile_update(TaskState* ts, int ntask, Elems E, Elems B, int* big_left) {
+    for (int t = int(blockIdx.x) * blockDim.x + threadIdx.x; t < ntask; t += gridDim.x * blockDim.x) {
+        TaskState& k = ts[t];
+        if (k.done) continue;
+        move(B, k.right, E, k.right);
+        const int np = k.left + k.L;
+        if (np == k.nth) k.done = 1;
+        else if (k.nth < np) k.right = np - 1;
+        else k.left = np + 1;
+        if (!k.done && k.left == k.right) k.done = 1;
+        if (!k.done && k.right - k.left + 1 > kBlockSelectMax) atomicAdd(big_left, 1);
+    }
+}
+
+__global__ void k_to_seltask(const TaskState* __restrict__ ts, int ntask, SelTask* out) {
+    for (int t = int(blockIdx.x) * blockDim.x + threadIdx.x; t < ntask; t += gridDim.x * blockDim.x) {
+        const TaskState& k = ts[t];
+        out[t] = SelTask{k.left, k.done ? k.left : k.right + 1, k.nth, k.axis, k.up};
     }
 }
 
@@ -525,6 +713,45 @@ int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaS
             if (phase->empty()) continue;
             DevBuf<SelTask> dt;
             D3G_TRY(upload(*phase, dt, s));
+            int longest = 0;
+            for (const SelTask& t : *phase) longest = std::max(longest, t.end - t.left);
+            if (longest > kBlockSelectMax) {
+                // Whole-GPU passes until every task fits a block.
+                const int nt = int(phase->size());
+                std::vector<TaskState> hs(static_cast<size_t>(nt));
+                for (int i = 0; i < nt; ++i) {
+                    const SelTask& t = (*phase)[size_t(i)];
+                    hs[size_t(i)] = TaskState{t.left, t.end - 1, t.nth, t.axis, t.up, t.end - t.left < 2 ? 1 : 0,
+                                              0.0, 0, 0, 0};
+                }
+                DevBuf<TaskState> dts;
+                DevBuf<int> ctrl, tiles;
+                D3G_TRY(upload(hs, dts, s));
+                D3G_TRY(ctrl.alloc(2, s));
+                D3G_TRY(tiles.alloc(size_t(n / kTile + nt + 1), s));
+                const unsigned tg = unsigned(kNumSMs * 8);
+                for (int iter = 0;; ++iter) {
+                    D3G_CUDA(cudaMemsetAsync(ctrl.p, 0, 2 * sizeof(int), s));
+                    k_plan<<<1, 1024, 0, s>>>(dts.p, nt, E, B, ctrl.p);
+                    k_tile_count<<<tg, kTileThreads, 0, s>>>(dts.p, nt, E, ctrl.p, tiles.p);
+                    k_tile_scan<<<1, 1024, 0, s>>>(dts.p, nt, ctrl.p, tiles.p);
+                    k_tile_scatter<<<tg, kTileThreads, 0, s>>>(dts.p, nt, E, B, ctrl.p, tiles.p, rk.p);
+                    k_tile_place<<<tg, kTileThreads, 0, s>>>(dts.p, nt, E, B, ctrl.p, rk.p);
+                    k_tile_pivot<<<grid_for(nt, 128), 128, 0, s>>>(dts.p, nt, E, B);
+                    k_tile_copy<<<tg, kTileThreads, 0, s>>>(dts.p, nt, E, B, ctrl.p);
+                    k_tile_update<<<grid_for(nt, 128), 128, 0, s>>>(dts.p, nt, E, B, ctrl.p + 1);
+                    D3G_CUDA(cudaGetLastError());
+                    int big_left = 0;
+                    D3G_CUDA(cudaMemcpyAsync(&big_left, ctrl.p + 1, sizeof big_left, cudaMemcpyDeviceToHost, s));
+                    D3G_CUDA(cudaStreamSynchronize(s));
+                    if (big_left == 0) break;
+                    if (iter > (1 << 26)) {
+                        set_error("spatial sort: quickselect did not converge");
+                        return D3G_ERR_INTERNAL;
+                    }
+                }
+                k_to_seltask<<<grid_for(nt, 128), 128, 0, s>>>(dts.p, nt, dt.p);
+            }
             k_select<<<unsigned(phase->size()), kSelThreads, 0, s>>>(dt.p, E, B, rk.p);
             D3G_CUDA(cudaGetLastError());
         }

@@ -58,3 +58,15 @@ def test_matches_oracle(cuda, case):
 def test_matches_reference_1e6(cuda):
     pts = d3.gen_uniform(1000000, 3)
     assert (d3.spatial_sort(pts) == oracle.ref_spatial_sort(pts)).all()
+
+
+def test_matches_reference_multiblock_4e6(cuda):
+    # Large enough that the top-level quickselects run as whole-GPU passes.
+    pts = d3.gen_uniform(4000000, 8)
+    assert (d3.spatial_sort(pts) == oracle.ref_spatial_sort(pts)).all()
+
+
+def test_matches_reference_lattice_duplicates_large(cuda):
+    # Many equal coordinates (long runs of ties in every quickselect).
+    pts = np.random.default_rng(9).integers(0, 40, (600000, 3)).astype(np.float64)
+    assert (d3.spatial_sort(pts) == oracle.ref_spatial_sort(pts)).all()
