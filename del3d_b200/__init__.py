@@ -81,6 +81,12 @@ class _Options(ctypes.Structure):
                 ("max_rounds", _I32), ("timing", _I32)]
 
 
+class _BatchResult(ctypes.Structure):
+    _fields_ = [("n_sets", _I32), ("cell_offsets", ctypes.POINTER(_I64)),
+                ("cells", ctypes.POINTER(_I32)), ("n_vertices", ctypes.POINTER(_I64)),
+                ("device_ms", ctypes.c_double), ("stats", BuildStats)]
+
+
 class _PredStats(ctypes.Structure):
     _fields_ = [("n_queries", _I64), ("n_exact", _I64)]
 
@@ -117,6 +123,12 @@ def library() -> ctypes.CDLL:
     lib.d3g_build_device.argtypes = [_P, _I64, ctypes.POINTER(_Options), _P, _I64,
                                      ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P,
                                      ctypes.POINTER(BuildStats)]
+    lib.d3g_build_batch.argtypes = [_P, _P, _I32, ctypes.POINTER(_Options), ctypes.POINTER(_BatchResult)]
+    lib.d3g_build_batch.restype = _INT
+    lib.d3g_batch_result_free.argtypes = [ctypes.POINTER(_BatchResult)]
+    lib.d3g_build_batch_device.argtypes = [_P, _P, _I32, ctypes.POINTER(_Options), _P, _I64, _P, _P, _P,
+                                           ctypes.POINTER(BuildStats)]
+    lib.d3g_build_batch_device.restype = _INT
     lib.d3g_gen_uniform.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, _P]
     lib.d3g_gen_sphere.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, _I32, _P]
     lib.d3g_gen_clusters.argtypes = [_I64, ctypes.c_uint32, _I32, ctypes.c_double, _P]
@@ -362,6 +374,65 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: 
     return out[: nc.value], nv.value
 
 
+def build_batch(sets, chunk: int = 0, stats: Optional[dict] = None):
+    """Builds many independent point sets in one call.  Returns, per set, its
+    finite cells ((k, 4) int32, indices local to the set, canonical order - the
+    same as Delaunay().build(set).finite_cells()) and its vertex count."""
+    lib = library()
+    arrays = [_points(a) for a in sets]
+    if not arrays:
+        return [], []
+    offs = np.zeros(len(arrays) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([a.shape[0] for a in arrays])
+    xyz = np.ascontiguousarray(np.concatenate(arrays) if offs[-1] else np.zeros((1, 3)))
+    opts = _Options()
+    lib.d3g_options_default(ctypes.byref(opts))
+    opts.chunk = int(chunk)
+    res = _BatchResult()
+    _check(lib.d3g_build_batch(_ptr(xyz), _ptr(offs), len(arrays), ctypes.byref(opts), ctypes.byref(res)),
+           "build_batch")
+    try:
+        co = np.ctypeslib.as_array(res.cell_offsets, shape=(len(arrays) + 1,)).copy()
+        nv = np.ctypeslib.as_array(res.n_vertices, shape=(len(arrays),)).copy()
+        total = int(co[-1])
+        cells = (np.ctypeslib.as_array(res.cells, shape=(total * 4,)).reshape(total, 4).copy()
+                 if total else np.zeros((0, 4), dtype=np.int32))
+        if stats is not None:
+            stats.update(res.stats.as_dict())
+            stats["device_ms"] = res.device_ms
+    finally:
+        lib.d3g_batch_result_free(ctypes.byref(res))
+    return [cells[co[i]:co[i + 1]] for i in range(len(arrays))], [int(v) for v in nv]
+
+
+def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk: int = 0,
+                       stats: Optional[dict] = None):
+    """Device-resident form of build_batch: `points_dev` (n, 3) float64 CUDA
+    tensor holding the sets back to back, `set_offsets` (n_sets + 1) host
+    int64.  Returns the device cells tensor (all sets), the cell offsets per
+    set and the vertex counts per set.  Synchronises `stream`."""
+    import torch
+
+    lib = library()
+    offs = np.ascontiguousarray(set_offsets, dtype=np.int64)
+    nsets = offs.shape[0] - 1
+    x = points_dev.contiguous()
+    if out is None:
+        out = torch.empty((8 * x.shape[0] + 64, 4), dtype=torch.int32, device=x.device)
+    co = np.zeros(nsets + 1, dtype=np.int64)
+    nv = np.zeros(nsets, dtype=np.int64)
+    opts = _Options()
+    lib.d3g_options_default(ctypes.byref(opts))
+    opts.chunk = int(chunk)
+    st = BuildStats()
+    _check(lib.d3g_build_batch_device(x.data_ptr(), _ptr(offs), nsets, ctypes.byref(opts), out.data_ptr(),
+                                      out.shape[0], _ptr(co), _ptr(nv), _P(stream), ctypes.byref(st)),
+           "build_batch_device")
+    if stats is not None:
+        stats.update(st.as_dict())
+    return out[: int(co[-1])], co, nv
+
+
 # ---- synthetic inputs -------------------------------------------------------------
 
 
@@ -396,3 +467,27 @@ def gen_lattice(n: int) -> np.ndarray:
     if n:
         library().d3g_gen_lattice(n, _ptr(out))
     return out
+
+
+DISTRIBUTIONS = ("uniform", "clusters", "lattice", "sphere")
+
+
+def gen_set(dist: str, n: int, seed: int) -> np.ndarray:
+    """One set of the mixed workloads: n points of `dist` from `seed`."""
+    if dist == "uniform":
+        return gen_uniform(n, seed)
+    if dist == "clusters":
+        return gen_clusters(n, seed, 8, 0.02)
+    if dist == "lattice":
+        return gen_lattice(n)
+    return gen_sphere(n, seed, 1.0, 1024, dedupe=True)
+
+
+def mixed_workload(n_sets: int, lo: int = 32, hi: int = 65536, seed: int = 2024, first_seed: int = 1000):
+    """The mixed batched workload: n_sets sets with sizes log-uniform in
+    [lo, hi] and a distribution drawn uniformly from DISTRIBUTIONS (both from
+    numpy's PCG64 with `seed`); set k's points come from mt19937(first_seed + k)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), n_sets))).astype(np.int64)
+    dists = rng.integers(0, len(DISTRIBUTIONS), n_sets)
+    return [gen_set(DISTRIBUTIONS[d], int(n), first_seed + k) for k, (n, d) in enumerate(zip(sizes, dists))]

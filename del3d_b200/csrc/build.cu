@@ -40,6 +40,8 @@
 namespace d3g {
 
 int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaStream_t s);
+int spatial_order_sets_device(const double* d_xyz, const int64_t* h_off, const int64_t* d_off, int nsets,
+                              int32_t* d_order, cudaStream_t s);
 int multiscale_bounds(int64_t n, int64_t* b, int cap);
 
 namespace {
@@ -104,6 +106,8 @@ struct Workers {
     int* fac;     // fac_cap boundary facets (tet * 4 + facet) per worker
     int4* st_v;   // fac_cap staged new tets per worker (vertices) ...
     int4* st_n;   // ... and neighbours
+    int* wset;        // set of each worker
+    const int4* skips; // per set: its first tet's vertices (inserted before the rounds)
     int cav_cap;
     int fac_cap;
     int n;
@@ -111,7 +115,6 @@ struct Workers {
 
 struct Round {
     const unsigned* round;    // current round number (device), set by k_round_begin
-    int skip[4];              // the initial tet's vertices (already inserted)
     int* counters;            // [0] active workers, [1] parked workers, [2] winners
     unsigned long long* sums; // [0] region tets, [1] boundary facets of the winners
     unsigned long long* totals; // [0] winners, [1] attempts, [2] rounds with work,
@@ -220,14 +223,15 @@ __device__ int walk_w(int t, const Pt& p, int pid, const Tables& T, const double
 
 /// Advances worker w to the next point of its chunk (walked cyclically from its
 /// start offset), skipping the initial tet's vertices; -1 when the chunk is done.
-__device__ int next_point(const Workers& W, int w, const int* skip) {
+__device__ int next_point(const Workers& W, int w) {
     const int b = W.beg[w], len = W.end[w] - b, off = W.off[w];
+    const int4 sk = W.skips[W.wset[w]];
     int done = W.done[w];
     int v = -1;
     while (done < len) {
         const int c = b + (off + done) % len;
         ++done;
-        if (c != skip[0] && c != skip[1] && c != skip[2] && c != skip[3]) {
+        if (c != sk.x && c != sk.y && c != sk.z && c != sk.w) {
             v = c;
             break;
         }
@@ -478,7 +482,7 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
         if (advanced) {
             W.last[w] = v;
             W.parked[w] = 0;
-            cur = next_point(W, w, R.skip);
+            cur = next_point(W, w);
         }
         if (cur >= 0 && W.parked[w]) atomicAdd(sh_count + 1, 1);     // waits for a big round
         else if (state != WS_DONE && cur >= 0) atomicAdd(sh_count, 1);
@@ -499,32 +503,47 @@ __global__ void k_collect_parked(Workers W, int* list, int* count) {
     if (W.parked[w] && W.cur[w] >= 0) list[atomicAdd(count, 1)] = w;
 }
 
-/// Workers of one level [lb, le): one chunk each.  Each starts at a scattered
-/// offset inside its chunk: chunks that are neighbours along the curve are
-/// mirror images of each other, and workers walking them in step would reach
-/// their common boundary together and keep colliding.
-__global__ void k_setup_level(Workers W, int lb, int le, int chunk, int plb, int ple, int4 skip4) {
+/// One set's share of a level: vertices [lb, le) (global ids) inserted by
+/// workers [w0, w0 + count) with chunks of `chunk`; [plb, ple) is the set's
+/// previous level.
+struct LevelDesc {
+    int set, lb, le, chunk, plb, ple, w0;
+};
+
+/// Workers of one level, one chunk each.  Each starts at a scattered offset
+/// inside its chunk: chunks that are neighbours along the curve are mirror
+/// images of each other, and workers walking them in step would reach their
+/// common boundary together and keep colliding.
+__global__ void k_setup_level(Workers W, const LevelDesc* __restrict__ ds, int nds) {
     const int w = int(blockIdx.x) * blockDim.x + threadIdx.x;
     if (w >= W.n) return;
-    const int b = lb + w * chunk;
-    const int e = min(le, b + chunk);
+    int lo = 0, hi = nds - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ds[mid].w0 <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    const LevelDesc d = ds[lo];
+    const int lw = w - d.w0;
+    const int b = d.lb + lw * d.chunk;
+    const int e = min(d.le, b + d.chunk);
     const int len = e - b;
-    const int off = len > 0 ? int((uint32_t(w) * 2654435761u >> 7) % uint32_t(len)) : 0;
+    const int off = len > 0 ? int((uint32_t(lw) * 2654435761u >> 7) % uint32_t(len)) : 0;
     W.beg[w] = b;
     W.end[w] = e;
     W.off[w] = off;
     W.parked[w] = 0;
     W.done[w] = 0;
     W.last[w] = -1;
-    const int skip[4] = {skip4.x, skip4.y, skip4.z, skip4.w};
-    next_point(W, w, skip);
+    W.wset[w] = d.set;
+    next_point(W, w);
     // The previous level is ordered along the same curve: the same fraction
     // along it lands near this worker's first point.
-    int g = skip4.x;
-    if (ple > plb) {
-        const double frac = (double(w) * chunk + off) / double(le - lb);
-        g = plb + int(frac * double(ple - plb));
-        if (g >= ple) g = ple - 1;
+    int g = W.skips[d.set].x;
+    if (d.ple > d.plb) {
+        const double frac = (double(lw) * d.chunk + off) / double(d.le - d.lb);
+        g = d.plb + int(frac * double(d.ple - d.plb));
+        if (g >= d.ple) g = d.ple - 1;
     }
     W.guide[w] = g;
     W.state[w] = WS_DONE;
@@ -538,130 +557,189 @@ __global__ void k_check_finite(const double* __restrict__ xyz, int64_t n3, uint3
         if (!isfinite(xyz[i])) atomicOr(bad, 1u);
 }
 
+/// The set holding position g: off[s] <= g < off[s+1].
+__device__ __forceinline__ int set_of(const int64_t* __restrict__ off, int nsets, int64_t g) {
+    int lo = 0, hi = nsets - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+/// Global index of the input point at rank r (position r of its set's order).
+__device__ __forceinline__ int64_t point_at(const int32_t* __restrict__ order, const int64_t* __restrict__ off,
+                                            int nsets, int64_t r) {
+    return off[set_of(off, nsets, r)] + order[r];
+}
+
 /// Coordinate bit patterns (with -0.0 folded onto +0.0, which compare equal)
-/// of the point at each rank, for the duplicate grouping.
+/// of the point at each rank, for the duplicate grouping; axis 3 = the set.
 __global__ void k_coord_keys(const double* __restrict__ xyz, const int32_t* __restrict__ order,
-                             int64_t n, int axis, unsigned long long* __restrict__ keys,
-                             const int32_t* __restrict__ ranks) {
+                             const int64_t* __restrict__ off, int nsets, int64_t n, int axis,
+                             unsigned long long* __restrict__ keys, const int32_t* __restrict__ ranks) {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += int64_t(gridDim.x) * blockDim.x) {
-        const double x = xyz[3 * int64_t(order[ranks[i]]) + axis];
+        if (axis == 3) {
+            keys[i] = (unsigned long long)set_of(off, nsets, ranks[i]);
+            continue;
+        }
+        const double x = xyz[3 * point_at(order, off, nsets, ranks[i]) + axis];
         keys[i] = x == 0.0 ? 0ull : (unsigned long long)__double_as_longlong(x);
     }
 }
 
-__device__ __forceinline__ bool same_point(const double* xyz, int32_t i, int32_t j) {
-    const double* a = xyz + 3 * int64_t(i);
-    const double* b = xyz + 3 * int64_t(j);
+__device__ __forceinline__ bool same_point(const double* xyz, int64_t i, int64_t j) {
+    const double* a = xyz + 3 * i;
+    const double* b = xyz + 3 * j;
     return a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
 }
 
-/// Over ranks sorted by coordinates (ties by rank): flags the first rank of
-/// each group of equal points and records the group's representative, the
-/// point with the LAST rank (src/triangulation.cpp:77-81).
+/// Over ranks sorted by (set, coordinates), ties by rank: flags the first rank
+/// of each group of equal points of one set and records the group's
+/// representative, the point with the LAST rank (src/triangulation.cpp:77-81),
+/// as an index local to its set.
 __global__ void k_groups(const double* __restrict__ xyz, const int32_t* __restrict__ order,
-                         const int32_t* __restrict__ sranks, int64_t n, int32_t* __restrict__ first,
-                         int32_t* __restrict__ rep_at_first, int* ndup) {
+                         const int64_t* __restrict__ off, int nsets, const int32_t* __restrict__ sranks,
+                         int64_t n, int32_t* __restrict__ first, int32_t* __restrict__ rep_at_first,
+                         int* ndup) {
     for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < n;
          s += int64_t(gridDim.x) * blockDim.x) {
         const int32_t r = sranks[s];
-        const bool starts = s == 0 || !same_point(xyz, order[sranks[s - 1]], order[r]);
-        if (!starts) {
+        const int set = set_of(off, nsets, r);
+        const int64_t pr = off[set] + order[r];
+        auto same = [&](int64_t t) {
+            const int32_t rt = sranks[t];
+            const int st = set_of(off, nsets, rt);
+            return st == set && same_point(xyz, off[st] + order[rt], pr);
+        };
+        if (s > 0 && same(s - 1)) {
             first[r] = 0;
             atomicAdd(ndup, 1);
             continue;
         }
         int64_t e = s;
-        while (e + 1 < n && same_point(xyz, order[sranks[e + 1]], order[r])) ++e;
+        while (e + 1 < n && same(e + 1)) ++e;
         first[r] = 1;
         rep_at_first[r] = order[sranks[e]];
     }
 }
 
+/// Vertex records: coordinates, the input index (local to the set) the vertex
+/// stands for, and its set.
 __global__ void k_vertices(const double* __restrict__ xyz, const int32_t* __restrict__ order,
+                           const int64_t* __restrict__ off, int nsets,
                            const int32_t* __restrict__ first, const int32_t* __restrict__ vid_of_rank,
                            const int32_t* __restrict__ rep_at_first, int64_t n, bool dups,
-                           double* __restrict__ vx, int32_t* __restrict__ vert_point) {
+                           double* __restrict__ vx, int32_t* __restrict__ vert_point,
+                           int32_t* __restrict__ vset) {
     for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
          r += int64_t(gridDim.x) * blockDim.x) {
         if (dups && !first[r]) continue;
         const int32_t v = dups ? vid_of_rank[r] : int32_t(r);
-        const int32_t i = order[r];
-        vx[3 * int64_t(v)] = xyz[3 * int64_t(i)];
-        vx[3 * int64_t(v) + 1] = xyz[3 * int64_t(i) + 1];
-        vx[3 * int64_t(v) + 2] = xyz[3 * int64_t(i) + 2];
-        vert_point[v] = dups ? rep_at_first[r] : i;
+        const int set = set_of(off, nsets, r);
+        const int64_t i = off[set] + order[r];
+        vx[3 * int64_t(v)] = xyz[3 * i];
+        vx[3 * int64_t(v) + 1] = xyz[3 * i + 1];
+        vx[3 * int64_t(v) + 2] = xyz[3 * i + 2];
+        vert_point[v] = dups ? rep_at_first[r] : order[r];
+        vset[v] = set;
     }
 }
 
-__global__ void k_find_noncollinear(const double* __restrict__ vx, int nv, int* found, uint32_t* st) {
-    const Pt a = vpt(vx, 0), b = vpt(vx, 1);
-    for (int v = 2 + int(blockIdx.x) * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        if (v > *found) return;
-        if (!collinear(a, b, vpt(vx, v), st)) atomicMin(found, v);
+/// Per set: the first vertex (in insertion order) not collinear with its first
+/// two, and then the first not coplanar with those three.
+__global__ void k_find_noncollinear(const double* __restrict__ vx, int nv, const int32_t* __restrict__ vset,
+                                    const int32_t* __restrict__ voff, int* found, uint32_t* st) {
+    for (int v = int(blockIdx.x) * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const int set = vset[v], base = voff[set];
+        if (v - base < 2 || v > found[set]) continue;
+        if (!collinear(vpt(vx, base), vpt(vx, base + 1), vpt(vx, v), st)) atomicMin(found + set, v);
     }
 }
 
-__global__ void k_find_noncoplanar(const double* __restrict__ vx, int nv, int v2, int* found,
+__global__ void k_find_noncoplanar(const double* __restrict__ vx, int nv, const int32_t* __restrict__ vset,
+                                   const int32_t* __restrict__ voff, const int* found2, int* found3,
                                    uint32_t* st) {
-    const Pt a = vpt(vx, 0), b = vpt(vx, 1), c = vpt(vx, v2);
-    for (int v = 2 + int(blockIdx.x) * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-        if (v > *found) return;
-        if (v != v2 && orient3d(a, b, c, vpt(vx, v), st) != 0) atomicMin(found, v);
+    for (int v = int(blockIdx.x) * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const int set = vset[v], base = voff[set], v2 = found2[set];
+        if (v2 >= voff[set + 1] || v - base < 2 || v == v2 || v > found3[set]) continue;
+        if (orient3d(vpt(vx, base), vpt(vx, base + 1), vpt(vx, v2), vpt(vx, v), st) != 0)
+            atomicMin(found3 + set, v);
     }
 }
 
-/// One thread: the first tet and its four infinite neighbours.
-__global__ void k_init_tets(Tables T, const double* __restrict__ vx, int v0, int v1, int v2, int v3,
-                            uint32_t* st) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (orient3d(vpt(vx, v0), vpt(vx, v1), vpt(vx, v2), vpt(vx, v3), st) < 0) {
-        const int t = v0;
-        v0 = v1;
-        v1 = t;
+/// Per set: its first four vertices (or -1s when the set is flat: no cells,
+/// src/triangulation.cpp:943-949).
+__global__ void k_set_skips(const int32_t* __restrict__ voff, const int* found2, const int* found3,
+                            int nsets, int4* __restrict__ skips) {
+    for (int s = int(blockIdx.x) * blockDim.x + threadIdx.x; s < nsets; s += gridDim.x * blockDim.x) {
+        const int base = voff[s], end = voff[s + 1];
+        if (end - base >= 4 && found2[s] < end && found3[s] < end)
+            skips[s] = make_int4(base, base + 1, found2[s], found3[s]);
+        else
+            skips[s] = make_int4(-1, -1, -1, -1);
     }
-    int4 tv[5];
-    tv[0] = make_int4(v0, v1, v2, v3);
-    for (int i = 0; i < 4; ++i) {
-        // Facet i of the first tet, capped by the infinite vertex in slot i and
-        // two other slots swapped, so the cap is positively oriented.
-        int4 c = tv[0];
-        set_at(c, i, kInf);
-        const int a = (i + 1) & 3, b = (i + 2) & 3;
-        const int x = at(c, a);
-        set_at(c, a, at(c, b));
-        set_at(c, b, x);
-        tv[1 + i] = c;
-    }
-    int4 tn[5];
-    for (int t = 0; t < 5; ++t)
-        for (int f = 0; f < 4; ++f) {
-            int fv[3], w = 0;
-            for (int m = 0; m < 4; ++m)
-                if (m != f) fv[w++] = at(tv[t], m);
-            for (int u = 0; u < 5; ++u) {
-                if (u == t) continue;
-                for (int g = 0; g < 4; ++g) {
-                    int hits = 0;
-                    for (int m = 0; m < 4; ++m) {
-                        if (m == g) continue;
-                        const int x = at(tv[u], m);
-                        hits += (x == fv[0]) + (x == fv[1]) + (x == fv[2]);
+}
+
+/// One thread per set: the first tet and its four infinite neighbours, in
+/// slots 5s .. 5s+4.
+__global__ void k_init_tets(Tables T, const double* __restrict__ vx, const int4* __restrict__ skips,
+                            int nsets, uint32_t* st) {
+    for (int set = int(blockIdx.x) * blockDim.x + threadIdx.x; set < nsets; set += gridDim.x * blockDim.x) {
+        const int4 sk = skips[set];
+        if (sk.x < 0) continue;
+        int v0 = sk.x, v1 = sk.y;
+        const int v2 = sk.z, v3 = sk.w;
+        if (orient3d(vpt(vx, v0), vpt(vx, v1), vpt(vx, v2), vpt(vx, v3), st) < 0) {
+            const int t = v0;
+            v0 = v1;
+            v1 = t;
+        }
+        int4 tv[5];
+        tv[0] = make_int4(v0, v1, v2, v3);
+        for (int i = 0; i < 4; ++i) {
+            // Facet i of the first tet, capped by the infinite vertex in slot i
+            // and two other slots swapped, so the cap is positively oriented.
+            int4 c = tv[0];
+            set_at(c, i, kInf);
+            const int a = (i + 1) & 3, b = (i + 2) & 3;
+            const int x = at(c, a);
+            set_at(c, a, at(c, b));
+            set_at(c, b, x);
+            tv[1 + i] = c;
+        }
+        const int base = 5 * set;
+        int4 tn[5];
+        for (int t = 0; t < 5; ++t)
+            for (int f = 0; f < 4; ++f) {
+                int fv[3], w = 0;
+                for (int m = 0; m < 4; ++m)
+                    if (m != f) fv[w++] = at(tv[t], m);
+                for (int u = 0; u < 5; ++u) {
+                    if (u == t) continue;
+                    for (int g = 0; g < 4; ++g) {
+                        int hits = 0;
+                        for (int m = 0; m < 4; ++m) {
+                            if (m == g) continue;
+                            const int x = at(tv[u], m);
+                            hits += (x == fv[0]) + (x == fv[1]) + (x == fv[2]);
+                        }
+                        if (hits == 3) set_at(tn[t], f, (base + u) * 4 + g);
                     }
-                    if (hits == 3) set_at(tn[t], f, u * 4 + g);
                 }
             }
+        for (int t = 0; t < 5; ++t) {
+            T.tv[base + t] = tv[t];
+            T.tn[base + t] = tn[t];
+            T.alive[base + t] = 1;
         }
-    for (int t = 0; t < 5; ++t) {
-        T.tv[t] = tv[t];
-        T.tn[t] = tn[t];
-        T.alive[t] = 1;
+        T.vert_tet[v0] = base;
+        T.vert_tet[v1] = base;
+        T.vert_tet[v2] = base;
+        T.vert_tet[v3] = base;
     }
-    T.vert_tet[v0] = 0;
-    T.vert_tet[v1] = 0;
-    T.vert_tet[v2] = 0;
-    T.vert_tet[v3] = 0;
-    *T.tet_count = 5;
 }
 
 // ---- output -----------------------------------------------------------------------
@@ -694,12 +772,14 @@ __global__ void k_cell_flags(const int4* __restrict__ tv, const uint8_t* __restr
 /// plus their sort keys (shifted by one so the infinite vertex, -1, is 0).
 __global__ void k_cells_out(const int4* __restrict__ tv, const int32_t* __restrict__ flag,
                             const int32_t* __restrict__ pos, int ntet,
-                            const int32_t* __restrict__ vert_point, int kbits, int4* __restrict__ cells,
+                            const int32_t* __restrict__ vert_point, const int32_t* __restrict__ vset,
+                            int kbits, int4* __restrict__ cells,
                             unsigned long long* __restrict__ khi, unsigned long long* __restrict__ klo,
-                            int32_t* __restrict__ idx) {
+                            int32_t* __restrict__ idx, int32_t* __restrict__ cset) {
     for (int t = int(blockIdx.x) * blockDim.x + threadIdx.x; t < ntet; t += gridDim.x * blockDim.x) {
         if (!flag[t]) continue;
         const int4 c = tv[t];
+        if (cset) cset[pos[t]] = vset[c.x != kInf ? c.x : c.y];
         int4 q;
         q.x = c.x == kInf ? -1 : vert_point[c.x];
         q.y = c.y == kInf ? -1 : vert_point[c.y];
@@ -744,6 +824,13 @@ __global__ void k_gather_u64(const unsigned long long* __restrict__ in, const in
         o[i] = in[ix[i]];
 }
 
+__global__ void k_gather_i32(const int32_t* __restrict__ in, const int32_t* __restrict__ ix, int64_t m,
+                             int32_t* __restrict__ o) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+         i += int64_t(gridDim.x) * blockDim.x)
+        o[i] = in[ix[i]];
+}
+
 __global__ void k_iota32(int32_t* __restrict__ a, int64_t m) {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
          i += int64_t(gridDim.x) * blockDim.x)
@@ -758,13 +845,15 @@ __global__ void k_widen(const int32_t* __restrict__ a, int64_t m, int64_t* __res
 
 }  // namespace
 
-/// Device-resident result of one build.
+/// Device-resident result of one build of one or more sets.
 struct DeviceResult {
-    DevBuf<int4> cells;
-    DevBuf<int4> all;
-    DevBuf<int64_t> inc_off;
+    DevBuf<int4> cells;          // finite cells of every set, set by set, canonical order
+    DevBuf<int4> all;            // single set only: all cells
+    DevBuf<int64_t> inc_off;     // single set only: incident CSR
     DevBuf<int32_t> inc;
     int64_t n_cells = 0, n_all = 0, n_vertices = 0, n_inc = 0;
+    std::vector<int64_t> cell_off;   // per set: [cell_off[s], cell_off[s+1]) of `cells`
+    std::vector<int64_t> set_nv;     // per set: distinct points
     d3g_build_stats stats{};
     void reset() {
         cells.release();
@@ -772,29 +861,52 @@ struct DeviceResult {
         inc_off.release();
         inc.release();
         n_cells = n_all = n_vertices = n_inc = 0;
+        cell_off.clear();
+        set_nv.clear();
         stats = d3g_build_stats{};
     }
 };
 
 namespace {
 
-/// Sorts `n` canonical cells lexicographically into `out` (keys prepared by
-/// k_cells_out).
+__global__ void k_voff(const int64_t* __restrict__ off, int nsets, const int32_t* __restrict__ vid, bool dups,
+                       int64_t n, int nv, int32_t* __restrict__ voff) {
+    for (int s = int(blockIdx.x) * blockDim.x + threadIdx.x; s <= nsets; s += gridDim.x * blockDim.x) {
+        const int64_t o = off[s];
+        voff[s] = o >= n ? nv : (dups ? vid[o] : int32_t(o));
+    }
+}
+
+__global__ void k_count_sets(const int32_t* __restrict__ cset, int64_t n, int64_t* __restrict__ count) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x)
+        atomicAdd(reinterpret_cast<unsigned long long*>(count + cset[i]), 1ull);
+}
+
+/// Sorts `n` canonical cells lexicographically - by set first when `cset` is
+/// given - into `out` (keys prepared by k_cells_out).
 int sort_cells(DevBuf<int4>& cells, DevBuf<unsigned long long>& khi, DevBuf<unsigned long long>& klo,
-               DevBuf<int32_t>& idx, int64_t n, int kbits, DevBuf<int4>& out, cudaStream_t s) {
+               DevBuf<int32_t>& idx, const int32_t* cset, int nsets, int64_t n, int kbits,
+               DevBuf<int4>& out, cudaStream_t s) {
     D3G_TRY(out.alloc(size_t(n), s));
     if (n == 0) return D3G_OK;
-    DevBuf<unsigned long long> k2;
+    DevBuf<unsigned long long> k2, kg;
     DevBuf<int32_t> i2;
     D3G_TRY(k2.alloc(size_t(n), s));
+    D3G_TRY(kg.alloc(size_t(n), s));
     D3G_TRY(i2.alloc(size_t(n), s));
-    // LSD: low half first, then a stable sort on the high half.
+    // LSD: low half, then the high half, then (several sets) the set - each stable.
     D3G_TRY(sort_pairs(klo.p, k2.p, idx.p, i2.p, n, 0, 2 * kbits, s));
-    // Re-gather the high keys in that order, then sort by them.
-    DevBuf<unsigned long long> khi2;
-    D3G_TRY(khi2.alloc(size_t(n), s));
-    k_gather_u64<<<grid_for(n, 256), 256, 0, s>>>(khi.p, i2.p, n, khi2.p);
-    D3G_TRY(sort_pairs(khi2.p, k2.p, i2.p, idx.p, n, 0, 2 * kbits, s));
+    k_gather_u64<<<grid_for(n, 256), 256, 0, s>>>(khi.p, i2.p, n, kg.p);
+    D3G_TRY(sort_pairs(kg.p, k2.p, i2.p, idx.p, n, 0, 2 * kbits, s));
+    if (cset) {
+        DevBuf<int32_t> sk, sk2;
+        D3G_TRY(sk.alloc(size_t(n), s));
+        D3G_TRY(sk2.alloc(size_t(n), s));
+        k_gather_i32<<<grid_for(n, 256), 256, 0, s>>>(cset, idx.p, n, sk.p);
+        D3G_TRY(sort_pairs(sk.p, sk2.p, idx.p, i2.p, n, 0, bits_for(uint64_t(nsets)), s));
+        std::swap(idx.p, i2.p);
+    }
     k_gather_cells<<<grid_for(n, 256), 256, 0, s>>>(cells.p, idx.p, n, out.p);
     D3G_CUDA(cudaGetLastError());
     return D3G_OK;
@@ -802,8 +914,8 @@ int sort_cells(DevBuf<int4>& cells, DevBuf<unsigned long long>& khi, DevBuf<unsi
 
 }  // namespace
 
-int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
-                      DeviceResult& R);
+int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const d3g_options& opt,
+                    cudaStream_t s, DeviceResult& R);
 
 /// A non-blocking stream of the calling thread for the current device; it lives
 /// as long as the thread, so buffers bound to it can be freed at any later time.
@@ -819,10 +931,10 @@ cudaStream_t internal_stream() {
 /// Runs the build on `s`, or - for the legacy default stream, which cannot be
 /// captured into a graph - on the thread's internal stream, after the legacy
 /// stream's prior work (the build synchronises its stream before returning).
-int build_on_stream(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
-                    DeviceResult& R) {
+int build_on_stream(const double* d_xyz, const int64_t* h_off, int nsets, const d3g_options& opt,
+                    cudaStream_t s, DeviceResult& R) {
     D3G_TRY(prepare_device());
-    if (s != nullptr && s != cudaStreamLegacy) return build_device_impl(d_xyz, n, opt, s, R);
+    if (s != nullptr && s != cudaStreamLegacy) return build_sets_impl(d_xyz, h_off, nsets, opt, s, R);
     cudaStream_t own = internal_stream();
     if (!own) {
         set_error("d3g_build: could not create a stream");
@@ -833,21 +945,42 @@ int build_on_stream(const double* d_xyz, int64_t n, const d3g_options& opt, cuda
     cudaEventRecord(ev, cudaStreamLegacy);
     cudaStreamWaitEvent(own, ev, 0);
     cudaEventDestroy(ev);
-    return build_device_impl(d_xyz, n, opt, own, R);
+    return build_sets_impl(d_xyz, h_off, nsets, opt, own, R);
 }
 
-int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
-                      DeviceResult& R) {
+int build_on_stream(const double* d_xyz, int64_t n, const d3g_options& opt, cudaStream_t s,
+                    DeviceResult& R) {
+    const int64_t h_off[2] = {0, n};
+    return build_on_stream(d_xyz, h_off, 1, opt, s, R);
+}
+
+int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const d3g_options& opt,
+                    cudaStream_t s, DeviceResult& R) {
     R.reset();
+    const int64_t n = h_off[nsets];
+    int64_t max_n = 0;
+    for (int i = 0; i < nsets; ++i) {
+        if (h_off[i + 1] < h_off[i]) {
+            set_error("d3g_build: set offsets must not decrease");
+            return D3G_ERR_INVALID_ARGUMENT;
+        }
+        max_n = std::max<int64_t>(max_n, h_off[i + 1] - h_off[i]);
+    }
+    R.cell_off.assign(size_t(nsets) + 1, 0);
+    R.set_nv.assign(size_t(nsets), 0);
     if (n == 0) return D3G_OK;
-    if (n > (int64_t(1) << 27)) {
-        set_error("d3g_build: at most 2^27 points per set");
+    if (n > (int64_t(1) << 27) || h_off[0] != 0) {
+        set_error("d3g_build: at most 2^27 points per call, offsets starting at 0");
         return D3G_ERR_INVALID_ARGUMENT;
     }
+    const bool single = nsets == 1;
     const int N = int(n);
     DevBuf<uint32_t> status;
+    DevBuf<int64_t> d_off;
     D3G_TRY(status.alloc(4, s));
+    D3G_TRY(d_off.alloc(size_t(nsets) + 1, s));
     D3G_CUDA(cudaMemsetAsync(status.p, 0, 4 * sizeof(uint32_t), s));
+    D3G_CUDA(cudaMemcpyAsync(d_off.p, h_off, sizeof(int64_t) * (size_t(nsets) + 1), cudaMemcpyHostToDevice, s));
     k_check_finite<<<grid_for(3 * n, 256), 256, 0, s>>>(d_xyz, 3 * n, status.p + 1);
 
     cudaEvent_t ph[4];
@@ -862,11 +995,12 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     // ---- insertion order and duplicate groups ----
     DevBuf<int32_t> order;
     D3G_TRY(order.alloc(size_t(N), s));
-    D3G_TRY(spatial_order_device(d_xyz, n, order.p, s));
+    D3G_TRY(spatial_order_sets_device(d_xyz, h_off, d_off.p, nsets, order.p, s));
 
     DevBuf<double> vx;
-    DevBuf<int32_t> vert_point;
+    DevBuf<int32_t> vert_point, vset, voff;
     int nv = N;
+    D3G_TRY(voff.alloc(size_t(nsets) + 1, s));
     {
         DevBuf<int32_t> ranks, sranks, first, rep, vid;
         DevBuf<unsigned long long> keys, keys2;
@@ -878,31 +1012,40 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         D3G_TRY(ndup.alloc(1, s));
         D3G_CUDA(cudaMemsetAsync(ndup.p, 0, sizeof(int), s));
         k_iota32<<<grid_for(n, 256), 256, 0, s>>>(ranks.p, n);
-        // LSD over z, y, x: ranks sorted by coordinates, ties kept in rank order.
-        for (int axis = 2; axis >= 0; --axis) {
-            k_coord_keys<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, n, axis, keys.p, ranks.p);
-            D3G_TRY(sort_pairs(keys.p, keys2.p, ranks.p, sranks.p, n, 0, 64, s));
+        // LSD over z, y, x (and the set): ranks sorted by (set, coordinates),
+        // ties kept in rank order.
+        for (int axis = 2; axis >= (single ? 0 : -1); --axis) {
+            const int key_axis = axis < 0 ? 3 : axis;
+            k_coord_keys<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, d_off.p, nsets, n, key_axis, keys.p,
+                                                          ranks.p);
+            D3G_TRY(sort_pairs(keys.p, keys2.p, ranks.p, sranks.p, n, 0,
+                               key_axis == 3 ? bits_for(uint64_t(nsets)) : 64, s));
             std::swap(ranks.p, sranks.p);
         }
         D3G_TRY(first.alloc(size_t(N), s));
         D3G_TRY(rep.alloc(size_t(N), s));
-        k_groups<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, ranks.p, n, first.p, rep.p, ndup.p);
+        k_groups<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, d_off.p, nsets, ranks.p, n, first.p, rep.p,
+                                                  ndup.p);
         int hdup = 0;
         D3G_CUDA(cudaMemcpyAsync(&hdup, ndup.p, sizeof hdup, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaStreamSynchronize(s));
         nv = N - hdup;
         D3G_TRY(vx.alloc(size_t(3) * nv, s));
         D3G_TRY(vert_point.alloc(size_t(nv), s));
+        D3G_TRY(vset.alloc(size_t(nv), s));
         if (hdup > 0) {
             D3G_TRY(vid.alloc(size_t(N), s));
             D3G_TRY(exclusive_scan(first.p, vid.p, n, s));
         }
-        k_vertices<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, first.p, vid.p, rep.p, n, hdup > 0,
-                                                    vx.p, vert_point.p);
+        k_vertices<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, order.p, d_off.p, nsets, first.p, vid.p, rep.p, n,
+                                                    hdup > 0, vx.p, vert_point.p, vset.p);
+        k_voff<<<grid_for(nsets + 1, 128), 128, 0, s>>>(d_off.p, nsets, vid.p, hdup > 0, n, nv, voff.p);
         D3G_CUDA(cudaGetLastError());
     }
     order.release();
     R.n_vertices = nv;
+    std::vector<int32_t> hvoff(size_t(nsets) + 1);
+    D3G_CUDA(cudaMemcpyAsync(hvoff.data(), voff.p, sizeof(int32_t) * hvoff.size(), cudaMemcpyDeviceToHost, s));
 
     uint32_t hst[2] = {0, 0};
     D3G_CUDA(cudaMemcpyAsync(hst, status.p, sizeof hst, cudaMemcpyDeviceToHost, s));
@@ -911,43 +1054,42 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         set_error("d3g_build: non-finite coordinate");
         return D3G_ERR_INVALID_INPUT;
     }
+    for (int i = 0; i < nsets; ++i) R.set_nv[size_t(i)] = hvoff[size_t(i) + 1] - hvoff[size_t(i)];
 
     cudaEventRecord(ph[1], s);
-    // ---- the first tet: the first four affinely independent vertices ----
-    int v2 = -1, v3 = -1;
-    if (nv >= 4) {
-        DevBuf<int> found;
-        D3G_TRY(found.alloc(2, s));
-        k_set_int<<<1, 1, 0, s>>>(found.p, nv);
-        k_set_int<<<1, 1, 0, s>>>(found.p + 1, nv);
-        k_find_noncollinear<<<grid_for(nv, 256), 256, 0, s>>>(vx.p, nv, found.p, status.p);
-        int h = nv;
-        D3G_CUDA(cudaMemcpyAsync(&h, found.p, sizeof h, cudaMemcpyDeviceToHost, s));
-        D3G_CUDA(cudaStreamSynchronize(s));
-        if (h < nv) {
-            v2 = h;
-            k_find_noncoplanar<<<grid_for(nv, 256), 256, 0, s>>>(vx.p, nv, v2, found.p + 1, status.p);
-            D3G_CUDA(cudaMemcpyAsync(&h, found.p + 1, sizeof h, cudaMemcpyDeviceToHost, s));
-            D3G_CUDA(cudaStreamSynchronize(s));
-            if (h < nv) v3 = h;
-        }
-    }
-    if (v3 < 0) {
-        // Every point collinear or coplanar: no cells (src/triangulation.cpp:943-949).
-        D3G_CUDA(cudaMemcpyAsync(hst, status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        D3G_CUDA(cudaStreamSynchronize(s));
+    // ---- each set's first tet: its first four affinely independent vertices ----
+    DevBuf<int> found;
+    DevBuf<int4> skips;
+    D3G_TRY(found.alloc(2 * size_t(nsets), s));
+    D3G_TRY(skips.alloc(size_t(nsets), s));
+    D3G_CUDA(cudaMemsetAsync(found.p, 0x7F, 2 * sizeof(int) * size_t(nsets), s));
+    k_find_noncollinear<<<grid_for(nv, 256), 256, 0, s>>>(vx.p, nv, vset.p, voff.p, found.p, status.p);
+    k_find_noncoplanar<<<grid_for(nv, 256), 256, 0, s>>>(vx.p, nv, vset.p, voff.p, found.p, found.p + nsets,
+                                                         status.p);
+    k_set_skips<<<grid_for(nsets, 128), 128, 0, s>>>(voff.p, found.p, found.p + nsets, nsets, skips.p);
+    std::vector<int4> hskips(static_cast<size_t>(nsets));
+    D3G_CUDA(cudaMemcpyAsync(hskips.data(), skips.p, sizeof(int4) * size_t(nsets), cudaMemcpyDeviceToHost, s));
+    D3G_CUDA(cudaMemcpyAsync(hst, status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    D3G_CUDA(cudaStreamSynchronize(s));
+    {
         const int st = status_from_bits(hst[0]);
         if (st != D3G_OK) return st;
-        if (opt.want_incident) {
+    }
+    bool any_cells = false;
+    for (const int4& k : hskips) any_cells = any_cells || k.x >= 0;
+    if (!any_cells) {
+        // Every set collinear or coplanar: no cells (src/triangulation.cpp:943-949).
+        if (single && opt.want_incident) {
             D3G_TRY(R.inc_off.alloc(size_t(N) + 1, s));
             D3G_CUDA(cudaMemsetAsync(R.inc_off.p, 0, sizeof(int64_t) * (size_t(N) + 1), s));
         }
+        D3G_CUDA(cudaStreamSynchronize(s));
         return D3G_OK;
     }
 
     // ---- tables ----
     Tables T;
-    int64_t cap64 = int64_t(nv) * 8 + 4096;
+    int64_t cap64 = int64_t(nv) * 8 + 5 * int64_t(nsets) + 4096;
     if (cap64 > (int64_t(1) << 29)) cap64 = int64_t(1) << 29;
     T.cap = int(cap64);
     DevBuf<int4> tv, tn;
@@ -970,7 +1112,8 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     T.fnew = fnew.p;
     T.vert_tet = vert_tet.p;
     T.tet_count = tet_count.p;
-    k_init_tets<<<1, 32, 0, s>>>(T, vx.p, 0, 1, v2, v3, status.p);
+    k_set_int<<<1, 1, 0, s>>>(tet_count.p, 5 * nsets);
+    k_init_tets<<<grid_for(nsets, 64), 64, 0, s>>>(T, vx.p, skips.p, nsets, status.p);
 
     // ---- workers ----
     // A level of s points goes into a triangulation of p earlier points.  Two
@@ -978,10 +1121,10 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     // meet, so the useful number of simultaneous insertions grows with p, not
     // with s: each level gets about p / alpha workers (a fixed chunk if the
     // caller asks for one), each with a chunk of at least kMinChunk points.
+    // Several sets: their levels are aligned from the coarsest, and a round
+    // serves the workers of every set at once.
     const int alpha = opt.chunk < 0 ? -opt.chunk : 48;
     constexpr int kMinChunk = 16;
-    int64_t hb[64];
-    const int nb = multiscale_bounds(nv, hb, 63);
     auto level_chunk = [&](int64_t lb, int64_t le) -> int {
         if (opt.chunk > 0) return opt.chunk;
         const int64_t s_ = le - lb;
@@ -989,26 +1132,52 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         w_ = std::min<int64_t>(w_, (s_ + kMinChunk - 1) / kMinChunk);
         return int((s_ + w_ - 1) / w_);
     };
+    // levels[set] = bounds from the coarsest: [lev[k], lev[k+1]) local vertex ids.
+    std::vector<std::vector<int>> levels(static_cast<size_t>(nsets));
+    int nlev = 0;
+    for (int st = 0; st < nsets; ++st) {
+        if (hskips[size_t(st)].x < 0) continue;
+        int64_t hb[64];
+        const int nb = multiscale_bounds(R.set_nv[size_t(st)], hb, 63);
+        std::vector<int>& L = levels[size_t(st)];
+        L.push_back(0);
+        for (int k = nb - 1; k >= 0; --k) L.push_back(int(hb[k]));
+        nlev = std::max(nlev, int(L.size()) - 1);
+    }
+    auto level_descs = [&](int lev, std::vector<LevelDesc>& out) -> int {
+        out.clear();
+        int w = 0;
+        for (int st = 0; st < nsets; ++st) {
+            const std::vector<int>& L = levels[size_t(st)];
+            if (int(L.size()) - 1 <= lev) continue;
+            const int lb = L[size_t(lev)], le = L[size_t(lev) + 1];
+            if (le <= lb) continue;
+            const int plb = lev > 0 ? L[size_t(lev) - 1] : 0, ple = lb;
+            const int ch = level_chunk(lb, le);
+            const int base = hvoff[size_t(st)];
+            out.push_back(LevelDesc{st, base + lb, base + le, ch, base + plb, base + ple, w});
+            w += (le - lb + ch - 1) / ch;
+        }
+        return w;
+    };
     int maxw = 1;
-    for (int k = 0; k < nb; ++k) {
-        const int64_t lo = (k + 1 < nb) ? hb[k + 1] : 0;
-        const int64_t cnt = hb[k] - lo;
-        if (cnt <= 0) continue;
-        const int ch = level_chunk(lo, hb[k]);
-        maxw = std::max<int64_t>(maxw, (cnt + ch - 1) / ch);
+    {
+        std::vector<LevelDesc> tmp;
+        for (int lev = 0; lev < nlev; ++lev) maxw = std::max(maxw, level_descs(lev, tmp));
     }
     Workers W;
     W.cav_cap = kCavCap;
     W.fac_cap = kFacCap;
     W.n = maxw;
     DevBuf<int> wcur, wbeg, wend, woff, wdone, wlast, wguide, wstate, wncav, wnfac, wcav, wfac, counters;
-    DevBuf<int> wparked, blist, bcount, bcav, bfac;
+    DevBuf<int> wparked, wset, blist, bcount, bcav, bfac;
     DevBuf<int4> bsv, bsn;
     DevBuf<int4> wsv, wsn;
     D3G_TRY(wcur.alloc(size_t(maxw), s));
     D3G_TRY(wend.alloc(size_t(maxw), s));
     D3G_TRY(wbeg.alloc(size_t(maxw), s));
     D3G_TRY(wparked.alloc(size_t(maxw), s));
+    D3G_TRY(wset.alloc(size_t(maxw), s));
     D3G_TRY(woff.alloc(size_t(maxw), s));
     D3G_TRY(wdone.alloc(size_t(maxw), s));
     D3G_TRY(wlast.alloc(size_t(maxw), s));
@@ -1034,6 +1203,8 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     W.beg = wbeg.p;
     W.list = nullptr;
     W.parked = wparked.p;
+    W.wset = wset.p;
+    W.skips = skips.p;
     W.off = woff.p;
     W.done = wdone.p;
     W.last = wlast.p;
@@ -1047,10 +1218,6 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     W.st_n = wsn.p;
 
     Round Rd;
-    Rd.skip[0] = 0;
-    Rd.skip[1] = 1;
-    Rd.skip[2] = v2;
-    Rd.skip[3] = v3;
     Rd.counters = counters.p;
     Rd.sums = sums.p;
     Rd.totals = totals.p;
@@ -1071,8 +1238,6 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     } ev_guard{kev};
     // Big rounds: workers whose conflict region outgrew the normal scratch.
     Workers WB = W;
-    WB.cav_cap = kBigCav;
-    WB.fac_cap = kBigFac;
     auto big_rounds = [&]() -> int {
         if (!blist.p) {
             D3G_TRY(blist.alloc(size_t(maxw), s));
@@ -1130,15 +1295,10 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
             }
         }
     };
-    // Levels from the coarsest ([0, hb[nb-1])) to the finest ([hb[1], hb[0])).
-    for (int k = nb - 1; k >= 0; --k) {
-        const int lb = int(k + 1 < nb ? hb[k + 1] : 0);
-        const int le = int(hb[k]);
-        const int plb = int(k + 2 < nb ? hb[k + 2] : 0);
-        const int ple = lb;
-        if (le <= lb) continue;
-        const int chunk = level_chunk(lb, le);
-        W.n = (le - lb + chunk - 1) / chunk;
+    std::vector<LevelDesc> descs;
+    for (int lev = 0; lev < nlev; ++lev) {
+        W.n = level_descs(lev, descs);
+        if (W.n == 0) continue;
         const int round0 = round;
         long long won = 0, attempts = 0;
         long long won_before = 0, att_before = 0;
@@ -1155,8 +1315,10 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
             cudaEventCreate(&ev1);
             cudaEventRecord(ev0, s);
         }
-        k_setup_level<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, lb, le, chunk, plb, ple,
-                                                                  make_int4(0, 1, v2, v3));
+        DevBuf<LevelDesc> ddesc;
+        D3G_TRY(ddesc.alloc(descs.size(), s));
+        D3G_CUDA(cudaMemcpyAsync(ddesc.p, descs.data(), sizeof(LevelDesc) * descs.size(), cudaMemcpyHostToDevice, s));
+        k_setup_level<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, ddesc.p, int(descs.size()));
         const unsigned g = unsigned((int64_t(W.n) * 32 + 127) / 128);
         auto one_round = [&](bool timed) {
             k_round_begin<<<1, 1, 0, s>>>(Rd);
@@ -1237,8 +1399,8 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
             cudaEventSynchronize(ev1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev0, ev1);
-            fprintf(stderr, "d3g level [%d,%d) workers %d rounds %d inserted %lld attempts %lld ms %.2f\n",
-                    lb, le, W.n, round - round0, won, attempts, ms);
+            fprintf(stderr, "d3g level %d sets %zu workers %d rounds %d inserted %lld attempts %lld ms %.2f\n",
+                    lev, descs.size(), W.n, round - round0, won, attempts, ms);
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
         }
@@ -1266,10 +1428,10 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
     int ntet = 0;
     D3G_CUDA(cudaMemcpyAsync(&ntet, tet_count.p, sizeof ntet, cudaMemcpyDeviceToHost, s));
     D3G_CUDA(cudaStreamSynchronize(s));
-    const int kbits = bits_for(uint64_t(N) + 1);
-    for (int pass = 0; pass < (opt.want_all_cells ? 2 : 1); ++pass) {
+    const int kbits = bits_for(uint64_t(max_n) + 1);
+    for (int pass = 0; pass < (single && opt.want_all_cells ? 2 : 1); ++pass) {
         const bool with_inf = pass == 1;
-        DevBuf<int32_t> flag, pos, idx;
+        DevBuf<int32_t> flag, pos, idx, cset;
         D3G_TRY(flag.alloc(size_t(ntet), s));
         D3G_TRY(pos.alloc(size_t(ntet), s));
         k_cell_flags<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, alive.p, ntet, with_inf, flag.p);
@@ -1285,17 +1447,31 @@ int build_device_impl(const double* d_xyz, int64_t n, const d3g_options& opt, cu
         D3G_TRY(khi.alloc(size_t(nc), s));
         D3G_TRY(klo.alloc(size_t(nc), s));
         D3G_TRY(idx.alloc(size_t(nc), s));
-        k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, kbits,
-                                                        raw.p, khi.p, klo.p, idx.p);
+        if (!single) D3G_TRY(cset.alloc(size_t(nc), s));
+        k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, vset.p, kbits,
+                                                        raw.p, khi.p, klo.p, idx.p, single ? nullptr : cset.p);
         if (!with_inf) {
-            D3G_TRY(sort_cells(raw, khi, klo, idx, nc, kbits, R.cells, s));
+            D3G_TRY(sort_cells(raw, khi, klo, idx, single ? nullptr : cset.p, nsets, nc, kbits, R.cells, s));
             R.n_cells = nc;
+            if (single) {
+                R.cell_off[1] = nc;
+            } else {
+                DevBuf<int64_t> cnt, coff;
+                D3G_TRY(cnt.alloc(size_t(nsets) + 1, s));
+                D3G_TRY(coff.alloc(size_t(nsets) + 1, s));
+                D3G_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int64_t) * (size_t(nsets) + 1), s));
+                if (nc > 0) k_count_sets<<<grid_for(nc, 256), 256, 0, s>>>(cset.p, nc, cnt.p);
+                D3G_TRY(exclusive_scan(cnt.p, coff.p, int64_t(nsets) + 1, s));
+                D3G_CUDA(cudaMemcpyAsync(R.cell_off.data(), coff.p, sizeof(int64_t) * (size_t(nsets) + 1),
+                                         cudaMemcpyDeviceToHost, s));
+                D3G_CUDA(cudaStreamSynchronize(s));
+            }
         } else {
-            D3G_TRY(sort_cells(raw, khi, klo, idx, nc, kbits, R.all, s));
+            D3G_TRY(sort_cells(raw, khi, klo, idx, nullptr, 1, nc, kbits, R.all, s));
             R.n_all = nc;
         }
     }
-    if (opt.want_incident) {
+    if (single && opt.want_incident) {
         const int64_t m = 4 * R.n_cells;
         DevBuf<int32_t> pt, cell, pt2, cnt;
         D3G_TRY(R.inc_off.alloc(size_t(N) + 1, s));
@@ -1437,6 +1613,99 @@ int d3g_build_device(const double* d_xyz, int64_t n, const d3g_options* opts, in
     if (stats) *stats = R.stats;
     if (R.n_cells > cap_cells) {
         set_error("d3g_build_device: output capacity too small");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    if (R.n_cells > 0) {
+        if (!d_cells) return D3G_ERR_INVALID_ARGUMENT;
+        D3G_CUDA(cudaMemcpyAsync(d_cells, R.cells.p, sizeof(int4) * R.n_cells, cudaMemcpyDeviceToDevice, s));
+    }
+    R.reset();
+    D3G_CUDA(cudaStreamSynchronize(s));
+    return D3G_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+void d3g_batch_result_free(d3g_batch_result* r) {
+    if (!r) return;
+    free(r->cell_offsets);
+    free(r->cells);
+    free(r->n_vertices);
+    *r = d3g_batch_result{};
+}
+
+int d3g_build_batch(const double* xyz, const int64_t* set_offsets, int32_t n_sets, const d3g_options* opts,
+                    d3g_batch_result* out) {
+    if (!out || n_sets < 1 || !set_offsets) return D3G_ERR_INVALID_ARGUMENT;
+    *out = d3g_batch_result{};
+    const int64_t n = set_offsets[n_sets];
+    if (set_offsets[0] != 0 || n < 0 || (n > 0 && !xyz)) return D3G_ERR_INVALID_ARGUMENT;
+    d3g_options o;
+    d3g_options_default(&o);
+    if (opts) o = *opts;
+    D3G_TRY(ensure_device());
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st;
+    DeviceResult R;
+    {
+        DevBuf<double> dx;
+        D3G_TRY(dx.alloc(size_t(3 * (n > 0 ? n : 1)), s));
+        if (n > 0) D3G_CUDA(cudaMemcpyAsync(dx.p, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+        cudaEventRecord(e0, s);
+        st = build_on_stream(dx.p, set_offsets, n_sets, o, s, R);
+        cudaEventRecord(e1, s);
+    }
+    if (st == D3G_OK) {
+        out->n_sets = n_sets;
+        out->stats = R.stats;
+        out->cell_offsets = static_cast<int64_t*>(malloc(sizeof(int64_t) * (size_t(n_sets) + 1)));
+        out->n_vertices = static_cast<int64_t*>(malloc(sizeof(int64_t) * size_t(n_sets)));
+        out->cells = static_cast<int32_t*>(malloc(sizeof(int32_t) * 4 * size_t(R.n_cells > 0 ? R.n_cells : 1)));
+        for (int i = 0; i <= n_sets; ++i) out->cell_offsets[i] = R.cell_off[size_t(i)];
+        for (int i = 0; i < n_sets; ++i) out->n_vertices[i] = R.set_nv[size_t(i)];
+        if (R.n_cells > 0)
+            cudaMemcpyAsync(out->cells, R.cells.p, sizeof(int4) * R.n_cells, cudaMemcpyDeviceToHost, s);
+        const cudaError_t e = cudaStreamSynchronize(s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        out->device_ms = ms;
+        if (e != cudaSuccess) {
+            set_error(std::string("d3g_build_batch: ") + cudaGetErrorString(e));
+            st = D3G_ERR_CUDA;
+        }
+    }
+    R.reset();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != D3G_OK) d3g_batch_result_free(out);
+    return st;
+}
+
+int d3g_build_batch_device(const double* d_xyz, const int64_t* set_offsets, int32_t n_sets,
+                           const d3g_options* opts, int32_t* d_cells, int64_t cap_cells,
+                           int64_t* cell_offsets, int64_t* n_vertices, void* stream, d3g_build_stats* stats) {
+    if (n_sets < 1 || !set_offsets || cap_cells < 0) return D3G_ERR_INVALID_ARGUMENT;
+    if (set_offsets[0] != 0 || set_offsets[n_sets] < 0 || (set_offsets[n_sets] > 0 && !d_xyz))
+        return D3G_ERR_INVALID_ARGUMENT;
+    d3g_options o;
+    d3g_options_default(&o);
+    if (opts) o = *opts;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DeviceResult R;
+    const int st = build_on_stream(d_xyz, set_offsets, n_sets, o, s, R);
+    if (st != D3G_OK) return st;
+    if (cell_offsets)
+        for (int i = 0; i <= n_sets; ++i) cell_offsets[i] = R.cell_off[size_t(i)];
+    if (n_vertices)
+        for (int i = 0; i < n_sets; ++i) n_vertices[i] = R.set_nv[size_t(i)];
+    if (stats) *stats = R.stats;
+    if (R.n_cells > cap_cells) {
+        set_error("d3g_build_batch_device: output capacity too small");
         return D3G_ERR_INVALID_ARGUMENT;
     }
     if (R.n_cells > 0) {

@@ -153,6 +153,72 @@ __global__ void k_final(const int32_t* __restrict__ j, const int32_t* __restrict
     }
 }
 
+/// Index of the set holding global position g: offsets[s] <= g < offsets[s+1].
+__device__ __forceinline__ int set_of(const int64_t* __restrict__ off, int nsets, int64_t g) {
+    int lo = 0, hi = nsets - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+/// First and last position of each target in the steps sorted by target.
+__global__ void k_target_ranges(const int32_t* __restrict__ sj, int64_t cnt, int32_t* __restrict__ tfirst,
+                                int32_t* __restrict__ tlast) {
+    for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < cnt;
+         s += int64_t(gridDim.x) * blockDim.x) {
+        const int32_t q = sj[s];
+        if (s == 0 || sj[s - 1] != q) tfirst[q] = int32_t(s);
+        if (s + 1 == cnt || sj[s + 1] != q) tlast[q] = int32_t(s);
+    }
+}
+
+/// The shuffled sequence of every set at once.  All sets consume the same
+/// prefix of the one engine stream (seeded to 1 for each spatial_sort call),
+/// so the step targets j are shared; a set of n points stops at step n-1, which
+/// only changes which steps count as "later".
+__global__ void k_final_sets(const int32_t* __restrict__ j, const int32_t* __restrict__ pred,
+                             const int32_t* __restrict__ sm, const int32_t* __restrict__ tfirst,
+                             const int32_t* __restrict__ tlast, const int64_t* __restrict__ off,
+                             int nsets, int64_t total, int32_t* __restrict__ order) {
+    for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total;
+         g += int64_t(gridDim.x) * blockDim.x) {
+        const int s = set_of(off, nsets, g);
+        const int64_t p = g - off[s];
+        const int64_t n = off[s + 1] - off[s];
+        // The last step m < n that targets p.
+        int32_t l = -1;
+        int lo = tfirst[p], hi = tlast[p];
+        if (lo >= 0) {
+            while (lo <= hi) {
+                const int mid = (lo + hi) >> 1;
+                if (sm[mid] < n) {
+                    l = sm[mid];
+                    lo = mid + 1;
+                } else {
+                    hi = mid - 1;
+                }
+            }
+        }
+        if (l > p) {
+            order[g] = l;
+            continue;
+        }
+        int64_t x = p;
+        int32_t v = 0;
+        while (x > 0) {
+            const int32_t q = j[x];
+            if (q == x) { v = int32_t(x); break; }
+            const int32_t pm = pred[x];
+            if (pm > q) { v = pm; break; }
+            x = q;
+        }
+        order[g] = v;
+    }
+}
+
 // ---- the Hilbert median splits (spatial_sort.cpp:40-117) -------------------------
 //
 // Every split position is begin + (end - begin) / 2 whatever the data, so the
@@ -525,10 +591,11 @@ __global__ void __launch_bounds__(32) k_small_sort(const Seg* __restrict__ segs,
 }
 
 __global__ void k_gather_xyz(const double* __restrict__ xyz, const int32_t* __restrict__ order, int64_t n,
+                             const int64_t* __restrict__ off, int nsets,
                              double* __restrict__ x, double* __restrict__ y, double* __restrict__ z) {
     for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n;
          p += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t i = order[p];
+        const int64_t i = off[set_of(off, nsets, p)] + order[p];
         x[p] = xyz[3 * i];
         y[p] = xyz[3 * i + 1];
         z[p] = xyz[3 * i + 2];
@@ -537,14 +604,15 @@ __global__ void k_gather_xyz(const double* __restrict__ xyz, const int32_t* __re
 
 }  // namespace
 
-/// The reference's shuffled sequence (rand48.h:146-153 applied to 0..n-1).
-int shuffle_device(int64_t n, int32_t* d_order, cudaStream_t s) {
-    if (n <= 0) return D3G_OK;
-    if (n == 1) {
-        k_iota<<<1, 32, 0, s>>>(d_order, 1, 0);
-        D3G_CUDA(cudaGetLastError());
-        return D3G_OK;
-    }
+/// The reference's shuffled sequence (rand48.h:146-153 applied to 0..n-1) for
+/// every set: order[off[s] + p] is the local index at position p of set s.
+/// `h_off` / `d_off`: the same nsets+1 offsets on the host and on the device.
+int shuffle_sets_device(const int64_t* h_off, const int64_t* d_off, int nsets, int32_t* d_order,
+                        cudaStream_t s) {
+    int64_t n = 0;
+    for (int i = 0; i < nsets; ++i) n = std::max<int64_t>(n, h_off[i + 1] - h_off[i]);
+    const int64_t total = h_off[nsets] - h_off[0];
+    if (total <= 0) return D3G_OK;
     JumpTable jt;
     jt.step[0] = Affine{kA, kC};
     for (int i = 1; i < 48; ++i) jt.step[i] = compose(jt.step[i - 1], jt.step[i - 1]);
@@ -552,9 +620,9 @@ int shuffle_device(int64_t n, int32_t* d_order, cudaStream_t s) {
     // Expected rejections ~ n^2 / 2^32; draw with a generous margin, retry if short.
     int64_t margin = 1024 + 4 * (int64_t)((double(n) * double(n)) / 4294967296.0);
     for (int attempt = 0; attempt < 6; ++attempt, margin *= 4) {
-        const int64_t T = (n - 1) + margin;
+        const int64_t T = std::max<int64_t>(n - 1, 0) + margin;
         DevBuf<uint32_t> outs;
-        DevBuf<int32_t> cand, acc, j, keys2, vals, vals2, pred, last;
+        DevBuf<int32_t> cand, acc, j, keys2, vals, vals2, pred, tfirst, tlast;
         DevBuf<uint8_t> rej;
         DevBuf<unsigned long long> ncand;
         DevBuf<int64_t> nrej;
@@ -603,21 +671,38 @@ int shuffle_device(int64_t n, int32_t* d_order, cudaStream_t s) {
 
         // Steps m = 1..n-1 sorted by target j_m (stable: m ascending within a target).
         const int64_t cnt = n - 1;
-        D3G_TRY(keys2.alloc(size_t(cnt), s));
-        D3G_TRY(vals.alloc(size_t(cnt), s));
-        D3G_TRY(vals2.alloc(size_t(cnt), s));
-        k_iota<<<grid_for(cnt, 256), 256, 0, s>>>(vals.p, cnt, 1);
-        D3G_TRY(sort_pairs(j.p + 1, keys2.p, vals.p, vals2.p, cnt, 0, bits_for(uint64_t(n)), s));
         D3G_TRY(pred.alloc(size_t(n), s));
-        D3G_TRY(last.alloc(size_t(n), s));
-        D3G_CUDA(cudaMemsetAsync(last.p, 0xFF, sizeof(int32_t) * size_t(n), s));
-        k_lists<<<grid_for(cnt, 256), 256, 0, s>>>(keys2.p, vals2.p, cnt, pred.p, last.p);
-        k_final<<<grid_for(n, 256), 256, 0, s>>>(j.p, pred.p, last.p, n, d_order);
+        D3G_TRY(tfirst.alloc(size_t(n), s));
+        D3G_TRY(tlast.alloc(size_t(n), s));
+        D3G_CUDA(cudaMemsetAsync(tfirst.p, 0xFF, sizeof(int32_t) * size_t(n), s));
+        D3G_CUDA(cudaMemsetAsync(tlast.p, 0xFF, sizeof(int32_t) * size_t(n), s));
+        if (cnt > 0) {
+            D3G_TRY(keys2.alloc(size_t(cnt), s));
+            D3G_TRY(vals.alloc(size_t(cnt), s));
+            D3G_TRY(vals2.alloc(size_t(cnt), s));
+            k_iota<<<grid_for(cnt, 256), 256, 0, s>>>(vals.p, cnt, 1);
+            D3G_TRY(sort_pairs(j.p + 1, keys2.p, vals.p, vals2.p, cnt, 0, bits_for(uint64_t(n)), s));
+            DevBuf<int32_t> last_unused;
+            D3G_TRY(last_unused.alloc(size_t(n), s));
+            k_lists<<<grid_for(cnt, 256), 256, 0, s>>>(keys2.p, vals2.p, cnt, pred.p, last_unused.p);
+            k_target_ranges<<<grid_for(cnt, 256), 256, 0, s>>>(keys2.p, cnt, tfirst.p, tlast.p);
+        }
+        k_final_sets<<<grid_for(total, 256), 256, 0, s>>>(j.p, pred.p, vals2.p, tfirst.p, tlast.p, d_off,
+                                                          nsets, total, d_order);
         D3G_CUDA(cudaGetLastError());
         return D3G_OK;
     }
     set_error("shuffle: rejection margin exhausted");
     return D3G_ERR_INTERNAL;
+}
+
+int shuffle_device(int64_t n, int32_t* d_order, cudaStream_t s) {
+    if (n <= 0) return D3G_OK;
+    const int64_t h_off[2] = {0, n};
+    DevBuf<int64_t> d_off;
+    D3G_TRY(d_off.alloc(2, s));
+    D3G_CUDA(cudaMemcpyAsync(d_off.p, h_off, sizeof h_off, cudaMemcpyHostToDevice, s));
+    return shuffle_sets_device(h_off, d_off.p, 1, d_order, s);
 }
 
 /// Level boundaries of the multiscale pass: b[0] = n, b[k+1] = floor(b[k]/8)
@@ -644,22 +729,23 @@ int upload(const std::vector<T>& v, DevBuf<T>& d, cudaStream_t s) {
 
 }  // namespace
 
-int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaStream_t s) {
+/// spatial_sort of every set: d_order[off[s] + p] is the local index of the
+/// point at position p of set s's insertion order.
+int spatial_order_sets_device(const double* d_xyz, const int64_t* h_off, const int64_t* d_off, int nsets,
+                              int32_t* d_order, cudaStream_t s) {
+    const int64_t n = h_off[nsets] - h_off[0];
     if (n <= 0) return D3G_OK;
-    D3G_TRY(shuffle_device(n, d_order, s));
-    if (n < 2) return D3G_OK;
+    D3G_TRY(shuffle_sets_device(h_off, d_off, nsets, d_order, s));
     DevBuf<double> ex, ey, ez, bx, by, bz;
     DevBuf<int32_t> bidx, rk;
     D3G_TRY(ex.alloc(size_t(n), s));
     D3G_TRY(ey.alloc(size_t(n), s));
     D3G_TRY(ez.alloc(size_t(n), s));
-    k_gather_xyz<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, d_order, n, ex.p, ey.p, ez.p);
+    k_gather_xyz<<<grid_for(n, 256), 256, 0, s>>>(d_xyz, d_order, n, d_off, nsets, ex.p, ey.p, ez.p);
     const Elems E{d_order, ex.p, ey.p, ez.p};
 
-    // Roots: the multiscale levels (spatial_sort.cpp:130-137), each Hilbert-sorted
-    // from axis x with every direction "down".
-    int64_t hb[64];
-    const int nb = multiscale_bounds(n, hb, 63);
+    // Roots: each set's multiscale levels (spatial_sort.cpp:130-137), each
+    // Hilbert-sorted from axis x with every direction "down".
     std::vector<Seg> big, small;
     auto classify = [&](const Seg& g) {
         const int len = g.end - g.begin;
@@ -667,9 +753,15 @@ int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaS
         if (len <= kSmall) small.push_back(g);
         else big.push_back(g);
     };
-    for (int k = 0; k < nb; ++k) {
-        const int lo = int(k + 1 < nb ? hb[k + 1] : 0);
-        classify(Seg{lo, int(hb[k]), 0, 0, 0, 0});
+    for (int st = 0; st < nsets; ++st) {
+        const int64_t base = h_off[st], ns = h_off[st + 1] - h_off[st];
+        if (ns < 2) continue;
+        int64_t hb[64];
+        const int nb = multiscale_bounds(ns, hb, 63);
+        for (int k = 0; k < nb; ++k) {
+            const int64_t lo = k + 1 < nb ? hb[k + 1] : 0;
+            classify(Seg{int(base + lo), int(base + hb[k]), 0, 0, 0, 0});
+        }
     }
     if (!big.empty()) {
         D3G_TRY(bidx.alloc(size_t(n), s));
@@ -764,6 +856,15 @@ int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaS
         D3G_CUDA(cudaGetLastError());
     }
     return D3G_OK;
+}
+
+int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaStream_t s) {
+    if (n <= 0) return D3G_OK;
+    const int64_t h_off[2] = {0, n};
+    DevBuf<int64_t> d_off;
+    D3G_TRY(d_off.alloc(2, s));
+    D3G_CUDA(cudaMemcpyAsync(d_off.p, h_off, sizeof h_off, cudaMemcpyHostToDevice, s));
+    return spatial_order_sets_device(d_xyz, h_off, d_off.p, 1, d_order, s);
 }
 
 }  // namespace d3g

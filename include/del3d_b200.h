@@ -181,6 +181,33 @@ int d3g_build_device(const double* d_xyz, int64_t n, const d3g_options* opts, in
                      int64_t cap_cells, int64_t* n_cells_out, int64_t* n_vertices_out,
                      void* stream, d3g_build_stats* stats);
 
+/* ---- batched builds ------------------------------------------------------------
+ * Many independent point sets in one call (no reference counterpart: the
+ * reference builds one set per Delaunay::build call).  Set s is the points
+ * [set_offsets[s], set_offsets[s+1]) of `xyz`; set_offsets has n_sets + 1
+ * entries starting at 0.  Each set's cells are exactly what d3g_build returns
+ * for that set alone (same canonical order, indices local to the set). */
+typedef struct d3g_batch_result {
+    int32_t n_sets;
+    int64_t* cell_offsets;   /* n_sets + 1: set s owns cells [cell_offsets[s], cell_offsets[s+1]) */
+    int32_t* cells;          /* cell_offsets[n_sets] x 4                                          */
+    int64_t* n_vertices;     /* n_sets: distinct points per set                                  */
+    double device_ms;        /* device time of the build (CUDA events)                           */
+    d3g_build_stats stats;
+} d3g_batch_result;
+
+int d3g_build_batch(const double* xyz, const int64_t* set_offsets, int32_t n_sets, const d3g_options* opts,
+                    d3g_batch_result* out);
+void d3g_batch_result_free(d3g_batch_result* r);
+
+/* Device-resident points; set_offsets, cell_offsets (n_sets + 1) and n_vertices
+ * (n_sets) are host arrays; the cells of all sets go to d_cells (cap_cells x 4).
+ * Synchronises `stream`. */
+int d3g_build_batch_device(const double* d_xyz, const int64_t* set_offsets, int32_t n_sets,
+                           const d3g_options* opts, int32_t* d_cells, int64_t cap_cells,
+                           int64_t* cell_offsets, int64_t* n_vertices, void* stream,
+                           d3g_build_stats* stats);
+
 /* ---- synthetic inputs (host) -------------------------------------------------
  * Deterministic generators (std::mt19937 with u01 = word * 2^-32, written out). */
 void d3g_gen_uniform(int64_t n, uint32_t seed, double lo, double hi, double* xyz);
