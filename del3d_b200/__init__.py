@@ -78,7 +78,7 @@ class _Result(ctypes.Structure):
 
 class _Options(ctypes.Structure):
     _fields_ = [("want_all_cells", _I32), ("want_incident", _I32), ("chunk", _I32),
-                ("max_rounds", _I32), ("timing", _I32)]
+                ("max_rounds", _I32), ("timing", _I32), ("alpha_small", _I32), ("split", _I32)]
 
 
 class _BatchResult(ctypes.Structure):
@@ -347,7 +347,7 @@ class Delaunay:
 
 
 def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: bool = False,
-                 stats: Optional[dict] = None):
+                 stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0):
     """Builds from a device-resident torch tensor (n, 3) float64 on `stream`
     (a raw cudaStream_t handle; 0 = default) and returns the canonical finite
     cells as a device int32 tensor view (n_cells, 4) and the vertex count.
@@ -365,6 +365,8 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: 
     lib.d3g_options_default(ctypes.byref(opts))
     opts.chunk = int(chunk)
     opts.timing = int(timing)
+    opts.alpha_small = int(alpha_small)
+    opts.split = int(split)
     st = BuildStats()
     _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), out.shape[0],
                                 ctypes.byref(nc), ctypes.byref(nv), _P(stream), ctypes.byref(st)),
@@ -406,7 +408,7 @@ def build_batch(sets, chunk: int = 0, stats: Optional[dict] = None):
 
 
 def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk: int = 0,
-                       stats: Optional[dict] = None):
+                       stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0):
     """Device-resident form of build_batch: `points_dev` (n, 3) float64 CUDA
     tensor holding the sets back to back, `set_offsets` (n_sets + 1) host
     int64.  Returns the device cells tensor (all sets), the cell offsets per
@@ -424,6 +426,8 @@ def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
     opts.chunk = int(chunk)
+    opts.alpha_small = int(alpha_small)
+    opts.split = int(split)
     st = BuildStats()
     _check(lib.d3g_build_batch_device(x.data_ptr(), _ptr(offs), nsets, ctypes.byref(opts), out.data_ptr(),
                                       out.shape[0], _ptr(co), _ptr(nv), _P(stream), ctypes.byref(st)),

@@ -95,8 +95,9 @@ struct Workers {
     int* cur;     // current point (vertex id) of each worker
     int* beg;     // start of its chunk
     int* end;     // end of its chunk
-    int* off;     // where in the chunk it started (chunks are walked cyclically)
-    int* done;    // points of its chunk handled so far
+    int* pos;     // next position to visit, relative to beg (chunks are walked cyclically)
+    int* left;    // positions still to visit after the current point
+    int* nwon;    // points this worker inserted in the current level
     int* last;    // last vertex it inserted (-1: none yet)
     int* guide;   // an inserted vertex near its chunk, for the first walk
     int* state;
@@ -115,7 +116,8 @@ struct Workers {
 
 struct Round {
     const unsigned* round;    // current round number (device), set by k_round_begin
-    int* counters;            // [0] active workers, [1] parked workers, [2] winners
+    int* counters;            // [0] active workers, [1] parked workers, [2] winners,
+                              // [3] workers parked this round
     unsigned long long* sums; // [0] region tets, [1] boundary facets of the winners
     unsigned long long* totals; // [0] winners, [1] attempts, [2] rounds with work,
                                 // [3] parked workers, [4] stalled round seen, [5] active
@@ -132,7 +134,7 @@ __device__ __forceinline__ unsigned long long claim_key(const Round& R, int v) {
 __global__ void k_round_begin(Round R) {
     unsigned* r = const_cast<unsigned*>(R.round);
     *r += 1;
-    R.counters[0] = R.counters[1] = R.counters[2] = 0;
+    R.counters[0] = R.counters[1] = R.counters[2] = R.counters[3] = 0;
 }
 
 /// Folds one round's counters into the running totals; flags a round in which
@@ -143,7 +145,8 @@ __global__ void k_round_end(Round R) {
     R.totals[1] += (unsigned long long)(active + won);
     if (active + won > 0) R.totals[2] += 1;
     R.totals[3] = (unsigned long long)parked;
-    if (active > 0 && won == 0) R.totals[4] = 1;
+    // A worker parked this round may have claimed tets of every other candidate.
+    if (active > 0 && won == 0 && R.counters[3] == 0) R.totals[4] = 1;
     R.totals[5] = (unsigned long long)active;
 }
 
@@ -221,22 +224,24 @@ __device__ int walk_w(int t, const Pt& p, int pid, const Tables& T, const double
     return -1;
 }
 
-/// Advances worker w to the next point of its chunk (walked cyclically from its
-/// start offset), skipping the initial tet's vertices; -1 when the chunk is done.
+/// Advances worker w to the next point of its chunk (walked cyclically),
+/// skipping its set's first-tet vertices; -1 when the chunk is done.
 __device__ int next_point(const Workers& W, int w) {
-    const int b = W.beg[w], len = W.end[w] - b, off = W.off[w];
+    const int b = W.beg[w], len = W.end[w] - b;
     const int4 sk = W.skips[W.wset[w]];
-    int done = W.done[w];
+    int pos = W.pos[w], left = W.left[w];
     int v = -1;
-    while (done < len) {
-        const int c = b + (off + done) % len;
-        ++done;
+    while (left > 0) {
+        const int c = b + pos;
+        pos = pos + 1 == len ? 0 : pos + 1;
+        --left;
         if (c != sk.x && c != sk.y && c != sk.z && c != sk.w) {
             v = c;
             break;
         }
     }
-    W.done[w] = done;
+    W.pos[w] = pos;
+    W.left[w] = left;
     W.cur[w] = v;
     return v;
 }
@@ -330,6 +335,7 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
                 W.state[w] = WS_PARKED;
                 if (W.list) report(R.status, ST_CAVITY_CAPACITY);
                 else W.parked[w] = 1;
+                atomicAdd(R.counters + 3, 1);   // its claims may have blocked others
             }
             return;
         }
@@ -482,6 +488,7 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
         if (advanced) {
             W.last[w] = v;
             W.parked[w] = 0;
+            W.nwon[w] += 1;
             cur = next_point(W, w);
         }
         if (cur >= 0 && W.parked[w]) atomicAdd(sh_count + 1, 1);     // waits for a big round
@@ -531,9 +538,10 @@ __global__ void k_setup_level(Workers W, const LevelDesc* __restrict__ ds, int n
     const int off = len > 0 ? int((uint32_t(lw) * 2654435761u >> 7) % uint32_t(len)) : 0;
     W.beg[w] = b;
     W.end[w] = e;
-    W.off[w] = off;
+    W.pos[w] = off;
+    W.left[w] = len;
+    W.nwon[w] = 0;
     W.parked[w] = 0;
-    W.done[w] = 0;
     W.last[w] = -1;
     W.wset[w] = d.set;
     next_point(W, w);
@@ -547,6 +555,66 @@ __global__ void k_setup_level(Workers W, const LevelDesc* __restrict__ ds, int n
     }
     W.guide[w] = g;
     W.state[w] = WS_DONE;
+}
+
+// ---- growing the worker pool within a level ------------------------------------------
+//
+// A level's workers are sized for the points its set had when the level began;
+// by its end the set has 8 times as many.  Once a set's inserted points call
+// for twice its current workers, every worker of that set with enough of its
+// chunk left hands the second half of what remains to a new worker.
+
+struct SplitState {
+    int* set_p0;     // per set: points inserted before the level
+    int* set_ins;    // per set: points inserted so far in the level
+    int* set_w;      // per set: current workers
+    int* set_split;  // per set: split this time
+    int* nworkers;   // the pool size (device copy of W.n)
+    int cap;         // worker slots allocated
+};
+
+__global__ void k_count_wins(Workers W, SplitState S) {
+    const int w = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool ok = w < W.n;
+    const int set = ok ? W.wset[w] : -1;
+    const int c = ok ? W.nwon[w] : 0;
+    // Lanes of one set add once per warp.
+    const unsigned m = __match_any_sync(__activemask(), set);
+    const int sum = int(__reduce_add_sync(m, unsigned(c)));
+    if (ok && (threadIdx.x & 31) == __ffs(int(m)) - 1 && sum) atomicAdd(S.set_ins + set, sum);
+}
+
+__global__ void k_plan_split(SplitState S, int nsets, double alpha) {
+    for (int s = int(blockIdx.x) * blockDim.x + threadIdx.x; s < nsets; s += gridDim.x * blockDim.x) {
+        const double p = double(S.set_p0[s]) + double(S.set_ins[s]);
+        S.set_split[s] = (S.set_w[s] > 0 && p / alpha >= 2.0 * S.set_w[s]) ? 1 : 0;
+        S.set_ins[s] = 0;
+    }
+}
+
+__global__ void k_split(Workers W, SplitState S, int n_before) {
+    const int w = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (w >= n_before) return;
+    const int set = W.wset[w];
+    if (!S.set_split[set] || W.cur[w] < 0 || W.parked[w] || W.left[w] < 2 * 16) return;
+    const int slot = atomicAdd(S.nworkers, 1);
+    if (slot >= S.cap) return;
+    const int len = W.end[w] - W.beg[w];
+    const int left = W.left[w];
+    const int give = left - left / 2;
+    W.beg[slot] = W.beg[w];
+    W.end[slot] = W.end[w];
+    W.pos[slot] = (W.pos[w] + left / 2) % len;
+    W.left[slot] = give;
+    W.left[w] = left / 2;
+    W.nwon[slot] = 0;
+    W.parked[slot] = 0;
+    W.last[slot] = W.last[w];
+    W.guide[slot] = W.guide[w];
+    W.wset[slot] = set;
+    W.state[slot] = WS_DONE;
+    next_point(W, slot);
+    atomicAdd(S.set_w + set, 1);
 }
 
 // ---- set-up: validation, duplicates, initial tet ----------------------------------
@@ -877,10 +945,18 @@ __global__ void k_voff(const int64_t* __restrict__ off, int nsets, const int32_t
     }
 }
 
-__global__ void k_count_sets(const int32_t* __restrict__ cset, int64_t n, int64_t* __restrict__ count) {
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += int64_t(gridDim.x) * blockDim.x)
-        atomicAdd(reinterpret_cast<unsigned long long*>(count + cset[i]), 1ull);
+/// off[s] = first position of set s in the sorted set ids (lower bound).
+__global__ void k_set_bounds(const int32_t* __restrict__ sorted_set, int64_t n, int nsets,
+                             int64_t* __restrict__ off) {
+    for (int s = int(blockIdx.x) * blockDim.x + threadIdx.x; s <= nsets; s += gridDim.x * blockDim.x) {
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (sorted_set[mid] < s) lo = mid + 1;
+            else hi = mid;
+        }
+        off[s] = lo;
+    }
 }
 
 /// Sorts `n` canonical cells lexicographically - by set first when `cset` is
@@ -1125,10 +1201,15 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     // serves the workers of every set at once.
     const int alpha = opt.chunk < 0 ? -opt.chunk : 48;
     constexpr int kMinChunk = 16;
-    auto level_chunk = [&](int64_t lb, int64_t le) -> int {
+    // Below one latency wave of the GPU (about 4K resident warps), a round costs
+    // the same whatever its size: then a denser pool (down to one worker per
+    // kAlphaSmall earlier points) trades more collisions for far fewer rounds.
+    constexpr double kWaveWorkers = 4096.0;
+    const double kAlphaSmall = opt.alpha_small > 0 ? double(opt.alpha_small) : double(alpha);
+    auto level_chunk = [&](int64_t lb, int64_t le, double alpha_eff) -> int {
         if (opt.chunk > 0) return opt.chunk;
         const int64_t s_ = le - lb;
-        int64_t w_ = std::max<int64_t>(1, lb / alpha);
+        int64_t w_ = std::max<int64_t>(1, int64_t(double(lb) / alpha_eff));
         w_ = std::min<int64_t>(w_, (s_ + kMinChunk - 1) / kMinChunk);
         return int((s_ + w_ - 1) / w_);
     };
@@ -1144,7 +1225,19 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         for (int k = nb - 1; k >= 0; --k) L.push_back(int(hb[k]));
         nlev = std::max(nlev, int(L.size()) - 1);
     }
-    auto level_descs = [&](int lev, std::vector<LevelDesc>& out) -> int {
+    // The effective alpha of a level: alpha, lowered (to kAlphaSmall at most)
+    // while the whole pool would stay below one latency wave.
+    auto level_alpha = [&](int lev) -> double {
+        double w0 = 0;
+        for (int st = 0; st < nsets; ++st) {
+            const std::vector<int>& L = levels[size_t(st)];
+            if (int(L.size()) - 1 <= lev) continue;
+            w0 += std::max(1.0, double(L[size_t(lev)]) / alpha);
+        }
+        const double m = std::min(std::max(kWaveWorkers / std::max(w0, 1.0), 1.0), alpha / kAlphaSmall);
+        return alpha / m;
+    };
+    auto level_descs = [&](int lev, double alpha_eff, std::vector<LevelDesc>& out) -> int {
         out.clear();
         int w = 0;
         for (int st = 0; st < nsets; ++st) {
@@ -1153,7 +1246,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             const int lb = L[size_t(lev)], le = L[size_t(lev) + 1];
             if (le <= lb) continue;
             const int plb = lev > 0 ? L[size_t(lev) - 1] : 0, ple = lb;
-            const int ch = level_chunk(lb, le);
+            const int ch = level_chunk(lb, le, alpha_eff);
             const int base = hvoff[size_t(st)];
             out.push_back(LevelDesc{st, base + lb, base + le, ch, base + plb, base + ple, w});
             w += (le - lb + ch - 1) / ch;
@@ -1163,13 +1256,17 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     int maxw = 1;
     {
         std::vector<LevelDesc> tmp;
-        for (int lev = 0; lev < nlev; ++lev) maxw = std::max(maxw, level_descs(lev, tmp));
+        for (int lev = 0; lev < nlev; ++lev) maxw = std::max(maxw, level_descs(lev, level_alpha(lev), tmp));
     }
+    // Room for the pool to grow within levels (at most one worker per 16 points).
+    const bool grow = opt.chunk <= 0 && opt.split != 0;
+    if (grow) maxw = std::max<int>(maxw, int(std::min<int64_t>(int64_t(nv) / 16, int64_t(1) << 18)));
     Workers W;
     W.cav_cap = kCavCap;
     W.fac_cap = kFacCap;
     W.n = maxw;
-    DevBuf<int> wcur, wbeg, wend, woff, wdone, wlast, wguide, wstate, wncav, wnfac, wcav, wfac, counters;
+    DevBuf<int> wcur, wbeg, wend, wpos, wleft, wnwon, wlast, wguide, wstate, wncav, wnfac, wcav, wfac, counters;
+    DevBuf<int> set_p0, set_ins, set_w, set_split, nworkers;
     DevBuf<int> wparked, wset, blist, bcount, bcav, bfac;
     DevBuf<int4> bsv, bsn;
     DevBuf<int4> wsv, wsn;
@@ -1178,8 +1275,16 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     D3G_TRY(wbeg.alloc(size_t(maxw), s));
     D3G_TRY(wparked.alloc(size_t(maxw), s));
     D3G_TRY(wset.alloc(size_t(maxw), s));
-    D3G_TRY(woff.alloc(size_t(maxw), s));
-    D3G_TRY(wdone.alloc(size_t(maxw), s));
+    D3G_TRY(wpos.alloc(size_t(maxw), s));
+    D3G_TRY(wleft.alloc(size_t(maxw), s));
+    D3G_TRY(wnwon.alloc(size_t(maxw), s));
+    D3G_TRY(set_p0.alloc(size_t(nsets), s));
+    D3G_TRY(set_ins.alloc(size_t(nsets), s));
+    D3G_TRY(set_w.alloc(size_t(nsets), s));
+    D3G_TRY(set_split.alloc(size_t(nsets), s));
+    D3G_TRY(nworkers.alloc(1, s));
+    D3G_CUDA(cudaMemsetAsync(set_ins.p, 0, sizeof(int) * size_t(nsets), s));
+    SplitState SS{set_p0.p, set_ins.p, set_w.p, set_split.p, nworkers.p, maxw};
     D3G_TRY(wlast.alloc(size_t(maxw), s));
     D3G_TRY(wguide.alloc(size_t(maxw), s));
     D3G_TRY(wstate.alloc(size_t(maxw), s));
@@ -1189,7 +1294,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     D3G_TRY(wfac.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(wsv.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(wsn.alloc(size_t(maxw) * W.fac_cap, s));
-    D3G_TRY(counters.alloc(3, s));
+    D3G_TRY(counters.alloc(4, s));
     DevBuf<unsigned long long> sums, totals;
     DevBuf<unsigned> dround;
     D3G_TRY(sums.alloc(2, s));
@@ -1205,8 +1310,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     W.parked = wparked.p;
     W.wset = wset.p;
     W.skips = skips.p;
-    W.off = woff.p;
-    W.done = wdone.p;
+    W.pos = wpos.p;
+    W.left = wleft.p;
+    W.nwon = wnwon.p;
     W.last = wlast.p;
     W.guide = wguide.p;
     W.state = wstate.p;
@@ -1296,9 +1402,21 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         }
     };
     std::vector<LevelDesc> descs;
+    std::vector<int> hp0(static_cast<size_t>(nsets)), hw(static_cast<size_t>(nsets));
     for (int lev = 0; lev < nlev; ++lev) {
-        W.n = level_descs(lev, descs);
+        const double alpha_eff = level_alpha(lev);
+        W.n = level_descs(lev, alpha_eff, descs);
         if (W.n == 0) continue;
+        std::fill(hp0.begin(), hp0.end(), 0);
+        std::fill(hw.begin(), hw.end(), 0);
+        for (size_t i = 0; i < descs.size(); ++i) {
+            const LevelDesc& d = descs[i];
+            hp0[size_t(d.set)] = d.lb - hvoff[size_t(d.set)];
+            hw[size_t(d.set)] = (i + 1 < descs.size() ? descs[i + 1].w0 : W.n) - d.w0;
+        }
+        D3G_CUDA(cudaMemcpyAsync(set_p0.p, hp0.data(), sizeof(int) * size_t(nsets), cudaMemcpyHostToDevice, s));
+        D3G_CUDA(cudaMemcpyAsync(set_w.p, hw.data(), sizeof(int) * size_t(nsets), cudaMemcpyHostToDevice, s));
+        k_set_int<<<1, 1, 0, s>>>(nworkers.p, W.n);
         const int round0 = round;
         long long won = 0, attempts = 0;
         long long won_before = 0, att_before = 0;
@@ -1319,7 +1437,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         D3G_TRY(ddesc.alloc(descs.size(), s));
         D3G_CUDA(cudaMemcpyAsync(ddesc.p, descs.data(), sizeof(LevelDesc) * descs.size(), cudaMemcpyHostToDevice, s));
         k_setup_level<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, ddesc.p, int(descs.size()));
-        const unsigned g = unsigned((int64_t(W.n) * 32 + 127) / 128);
+        unsigned g = unsigned((int64_t(W.n) * 32 + 127) / 128);
         auto one_round = [&](bool timed) {
             k_round_begin<<<1, 1, 0, s>>>(Rd);
             if (timed) cudaEventRecord(kev[0], s);
@@ -1335,7 +1453,16 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         // the counters once per batch.  Rounds after the level is done find no
         // active worker and return at once.
         cudaGraphExec_t gexec = nullptr;
-        if (!opt.timing) {
+        struct GraphGuard {
+            cudaGraphExec_t* g;
+            ~GraphGuard() {
+                if (*g) cudaGraphExecDestroy(*g);
+            }
+        } graph_guard{&gexec};
+        auto capture = [&]() -> int {
+            if (gexec) cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+            if (opt.timing) return D3G_OK;
             cudaGraph_t graph = nullptr;
             D3G_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             for (int r = 0; r < kRoundsPerBatch; ++r) one_round(false);
@@ -1346,13 +1473,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ge));
                 return D3G_ERR_CUDA;
             }
-        }
-        struct GraphGuard {
-            cudaGraphExec_t* g;
-            ~GraphGuard() {
-                if (*g) cudaGraphExecDestroy(*g);
-            }
-        } graph_guard{&gexec};
+            return D3G_OK;
+        };
+        D3G_TRY(capture());
         for (;;) {
             const int batch = opt.timing ? 1 : kRoundsPerBatch;
             round += batch;
@@ -1362,11 +1485,27 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             }
             if (opt.timing) one_round(true);
             else D3G_CUDA(cudaGraphLaunch(gexec, s));
+            if (grow) {
+                D3G_CUDA(cudaMemsetAsync(set_ins.p, 0, sizeof(int) * size_t(nsets), s));
+                k_count_wins<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, SS);
+                k_plan_split<<<grid_for(nsets, 128), 128, 0, s>>>(SS, nsets, alpha_eff);
+                k_split<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, SS, W.n);
+            }
             unsigned long long ht[6];
             uint32_t hs = 0;
+            int hn = W.n;
             D3G_CUDA(cudaMemcpyAsync(ht, totals.p, sizeof ht, cudaMemcpyDeviceToHost, s));
             D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+            if (grow) D3G_CUDA(cudaMemcpyAsync(&hn, nworkers.p, sizeof hn, cudaMemcpyDeviceToHost, s));
             D3G_CUDA(cudaStreamSynchronize(s));
+            hn = std::min(hn, maxw);
+            if (hn != W.n) {
+                // The pool grew: the next batches serve the new workers too.
+                W.n = hn;
+                k_set_int<<<1, 1, 0, s>>>(nworkers.p, W.n);
+                g = unsigned((int64_t(W.n) * 32 + 127) / 128);
+                D3G_TRY(capture());
+            }
             if (hs != 0) {
                 const int st = status_from_bits(hs);
                 if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");
@@ -1456,12 +1595,12 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             if (single) {
                 R.cell_off[1] = nc;
             } else {
-                DevBuf<int64_t> cnt, coff;
-                D3G_TRY(cnt.alloc(size_t(nsets) + 1, s));
+                DevBuf<int64_t> coff;
+                DevBuf<int32_t> sorted_set;
                 D3G_TRY(coff.alloc(size_t(nsets) + 1, s));
-                D3G_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int64_t) * (size_t(nsets) + 1), s));
-                if (nc > 0) k_count_sets<<<grid_for(nc, 256), 256, 0, s>>>(cset.p, nc, cnt.p);
-                D3G_TRY(exclusive_scan(cnt.p, coff.p, int64_t(nsets) + 1, s));
+                D3G_TRY(sorted_set.alloc(size_t(nc > 0 ? nc : 1), s));
+                if (nc > 0) k_gather_i32<<<grid_for(nc, 256), 256, 0, s>>>(cset.p, idx.p, nc, sorted_set.p);
+                k_set_bounds<<<grid_for(nsets + 1, 128), 128, 0, s>>>(sorted_set.p, nc, nsets, coff.p);
                 D3G_CUDA(cudaMemcpyAsync(R.cell_off.data(), coff.p, sizeof(int64_t) * (size_t(nsets) + 1),
                                          cudaMemcpyDeviceToHost, s));
                 D3G_CUDA(cudaStreamSynchronize(s));
@@ -1521,6 +1660,8 @@ void d3g_options_default(d3g_options* o) {
     o->chunk = 0;
     o->max_rounds = 0;
     o->timing = 0;
+    o->alpha_small = 24;
+    o->split = 0;
 }
 
 void d3g_result_free(d3g_result* r) {

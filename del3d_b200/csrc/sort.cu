@@ -21,6 +21,8 @@
 #include "device_util.cuh"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 namespace d3g {
@@ -735,7 +737,14 @@ int spatial_order_sets_device(const double* d_xyz, const int64_t* h_off, const i
                               int32_t* d_order, cudaStream_t s) {
     const int64_t n = h_off[nsets] - h_off[0];
     if (n <= 0) return D3G_OK;
+    const bool trace = getenv("D3G_TRACE") != nullptr;
+    cudaEvent_t tev[4];
+    if (trace) {
+        for (auto& e : tev) cudaEventCreate(&e);
+        cudaEventRecord(tev[0], s);
+    }
     D3G_TRY(shuffle_sets_device(h_off, d_off, nsets, d_order, s));
+    if (trace) cudaEventRecord(tev[1], s);
     DevBuf<double> ex, ey, ez, bx, by, bz;
     DevBuf<int32_t> bidx, rk;
     D3G_TRY(ex.alloc(size_t(n), s));
@@ -849,11 +858,23 @@ int spatial_order_sets_device(const double* d_xyz, const int64_t* h_off, const i
         }
         big.swap(next);
     }
+    if (trace) cudaEventRecord(tev[2], s);
     if (!small.empty()) {
         DevBuf<Seg> ds;
         D3G_TRY(upload(small, ds, s));
         k_small_sort<<<unsigned(small.size()), 32, 0, s>>>(ds.p, E);
         D3G_CUDA(cudaGetLastError());
+    }
+    if (trace) {
+        cudaEventRecord(tev[3], s);
+        cudaEventSynchronize(tev[3]);
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, tev[0], tev[1]);
+        cudaEventElapsedTime(&b, tev[1], tev[2]);
+        cudaEventElapsedTime(&c, tev[2], tev[3]);
+        fprintf(stderr, "d3g sort: shuffle %.2f ms, big splits %.2f ms, small ranges %.2f ms (%zu)\n", a, b, c,
+                small.size());
+        for (auto& e : tev) cudaEventDestroy(e);
     }
     return D3G_OK;
 }

@@ -133,6 +133,12 @@ typedef struct d3g_options {
                              /* worker per alpha earlier points; 0 = default    */
     int32_t max_rounds;      /* 0 = default                                      */
     int32_t timing;          /* time each insertion kernel with CUDA events      */
+    int32_t alpha_small;     /* > 0: densest worker pool (one per alpha_small    */
+                             /* earlier points) while a round's pool stays below */
+                             /* one latency wave of the GPU; 0 = never denser;   */
+                             /* default 24                                       */
+    int32_t split;           /* grow the worker pool within a level as points go */
+                             /* in (0 = off)                                     */
 } d3g_options;
 
 /* What a build did (filled by d3g_build and d3g_build_device). */
