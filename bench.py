@@ -1,41 +1,60 @@
 #!/usr/bin/env python
 """Benchmark of the del3d Delaunay::build hot path on B200.
 
-Workload: one plain single-set build per step of 1e7 points i.i.d. uniform in
-[0,1)^3 (std::mt19937, u01 = word * 2^-32; seed 6 + rank), float64.  With
-N > 1 GPUs each rank builds its own set (replicas, weak scaling); there is no
-exchange step in a Delaunay build of independent sets.
+Workload (one step): the mixed batched workload - 4096 independent point sets,
+sizes log-uniform in [32, 65536], each drawn with equal probability from the
+uniform cube [0,1)^3, 8 Gaussian clusters (sigma 0.02), the integer lattice or
+the unit sphere quantised to a 2^-10 grid (duplicates removed), float64, per-set
+seeds (del3d_b200.mixed_workload).  All sets go to the GPU in one batched build
+(d3g_build_batch_device); every set's tet set is the reference's.  With N > 1
+GPUs each rank builds its own 4096 sets (weak scaling, no exchange step: sets
+are independent).
 
 One JSON line (rank 0):
-  value      points/s of the whole job, inputs resident in HBM, device-timed
-             with CUDA events on the build's stream (max over ranks);
-  e2e        the same metric through the host C ABI d3g_build (pinned host
-             input copied in, finite_cells + all_cells + incident_cells copied
-             back every step), which is what a del3d caller gets;
-  roofline   the dominant insertion kernel: algorithmic bytes it must touch
-             (live counts) / its event-timed duration, against measured HBM;
-  cpu_baseline  the reference del3d compiled from source, single thread, on a
-             1e6-point sample of the same distribution (rank 0, N = 1).
+  value       points/s of the whole job, inputs resident in HBM, device-timed
+              with CUDA events on the build's stream (max over ranks);
+  e2e         the same metric through the host C ABI d3g_build_batch: pinned
+              host input copied in, every set's finite cells copied back, each
+              step;
+  plain       the plain one-set-per-call GPU path (d3g_build_device) on a
+              1-in-8 sample of the same sets: points/s and per-set latency
+              p50/p99, and batched/plain;
+  latency     per-set latency of both forms (a batched set completes with its
+              batch);
+  roofline    the dominant insertion kernel: algorithmic bytes it must touch
+              (live counts) / its event-timed duration, against measured HBM;
+  cpu_baseline  the reference del3d compiled from source on a 1-in-16 sample of
+              the sets, one set per host thread.
+  plain_1e7   the plain path on 1e7 uniform points and the reference's
+              single-threaded build rate on 1e6 of them.
 
-`--impl reference` times the reference's own CPU build instead (rank 0 only).
+`--impl reference` times the reference's own CPU build on the same sample
+(rank 0 only; all host threads, one set per thread).
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "points/sec batched vs plain GPU at bit-exact tet sets; p50/p99 latency"
-N_POINTS = 10_000_000
-SEED = 6
-CPU_SAMPLE = 1_000_000
+N_SETS = 4096
+LO, HI = 32, 65536
+PLAIN_EVERY = 8
+CPU_EVERY = 16
+PLAIN_N = 10_000_000
+PLAIN_SEED = 6
+REF_PLAIN_SAMPLE = 1_000_000
 HBM_FALLBACK_GBS = 6650.0
 
 
@@ -45,9 +64,13 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=N_POINTS)
+    ap.add_argument("--sets", type=int, default=N_SETS)
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="warm-up and timed steps only (no other legs): the command profiled by ncu")
     return ap.parse_args()
 
 
@@ -59,11 +82,20 @@ def measured_peaks():
         return {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
 
 
-def workload(n):
-    return {"workload": f"plain single-set Delaunay build, {n:.0e} points uniform in [0,1)^3 "
-                        f"(mt19937 seed {SEED}+rank), float64",
-            "points_per_set": n, "sets_per_gpu_per_step": 1, "parallelism": "replicas",
-            "l2": "inputs larger than L2 (24 B/point points, ~57 B/tet tables)"}
+def workload_sets(n_sets, rank):
+    import del3d_b200 as d3
+
+    return d3.mixed_workload(n_sets, LO, HI, seed=2024 + rank, first_seed=1000 + n_sets * rank)
+
+
+def config(n_sets, n_points):
+    return {"workload": f"batched Delaunay builds: {n_sets} point sets, sizes log-uniform in "
+                        f"[{LO}, {HI}], uniform cube / 8-cluster Gaussian (sigma 0.02) / integer "
+                        f"lattice / quantised unit sphere (2^-10 grid, deduplicated), float64, "
+                        f"per-set seeds",
+            "sets_per_gpu_per_step": n_sets, "points_per_gpu_per_step": n_points,
+            "parallelism": "independent sets per GPU (replicas)",
+            "l2": "inputs larger than L2 (24 B/point, ~0.85 GB of points per step)"}
 
 
 class Clocks:
@@ -134,57 +166,168 @@ def count_launches(torch, fn):
         return None
 
 
-def cpu_baseline_leg():
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+# ---- the reference's CPU build (oracle/_ref: the reference compiled from its own sources) ----
+
+
+def reference_build_sets(sets, threads):
+    """Builds every set with the reference (one set per host thread at a time).
+    Returns (wall seconds, sum of per-set build seconds, points)."""
     import oracle
-    import del3d_b200 as d3
+
+    lib = oracle.ref()
+
+    def one(a):
+        nc = ctypes.c_int64(0)
+        return lib.ref_build_time(a.ctypes.data, a.shape[0], ctypes.byref(nc))
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        per_set = list(ex.map(one, sets))
+    wall = time.perf_counter() - t0
+    return wall, sum(per_set), sum(a.shape[0] for a in sets)
+
+
+def host_threads():
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return max(1, os.cpu_count() or 1)
+
+
+def cpu_sample(sets):
+    # Largest first so the thread pool does not end on one long set.
+    sample = sets[::CPU_EVERY]
+    return sorted(sample, key=lambda a: -a.shape[0])
+
+
+def cpu_baseline_leg(sets):
+    import oracle
 
     if not oracle.ref_available():
         return None
-    pts = d3.gen_uniform(CPU_SAMPLE, SEED)
-    import ctypes
-    import numpy as np
-
-    nc = ctypes.c_int64(0)
-    t = oracle.ref().ref_build_time(pts.ctypes.data, pts.shape[0], ctypes.byref(nc))
-    return {"value": CPU_SAMPLE / t, "unit": "points/s", "cores": 1, "kind": "reference",
-            "sample": f"one reference Delaunay::build of {CPU_SAMPLE:.0e} points of the same "
-                      f"distribution (seed {SEED}), {t:.2f} s, single-threaded as the reference is"}
+    sample = cpu_sample(sets)
+    threads = host_threads()
+    wall, cpu_s, pts = reference_build_sets(sample, threads)
+    return {"value": pts / wall, "unit": "points/s", "cores": threads, "kind": "reference",
+            "sample": f"every {CPU_EVERY}th set of the workload ({len(sample)} sets, {pts} points), "
+                      f"one set per thread on {threads} host threads; {wall:.2f} s wall, "
+                      f"{cpu_s:.2f} s of single-thread build time "
+                      f"({pts / cpu_s:.0f} points/s per thread)"}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import ctypes
-
-    import del3d_b200 as d3
     import oracle
 
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
         return 0
-    pts = d3.gen_uniform(CPU_SAMPLE, SEED)
-    nc = ctypes.c_int64(0)
-    times = []
+    sets = workload_sets(args.sets, 0)
+    sample = cpu_sample(sets)
+    threads = host_threads()
+    times, pts = [], 0
     for step in range(args.warmup + args.steps):
-        t = oracle.ref().ref_build_time(pts.ctypes.data, pts.shape[0], ctypes.byref(nc))
+        wall, _, pts = reference_build_sets(sample, threads)
         if step >= args.warmup:
-            times.append(t)
-    value = CPU_SAMPLE * len(times) / sum(times)
-    cfg = workload(args.n)
-    cfg["reference_sample"] = f"{CPU_SAMPLE:.0e} points per step (a bounded sample of the workload)"
+            times.append(wall)
+    value = pts * len(times) / sum(times)
+    cfg = config(args.sets, sum(a.shape[0] for a in sets))
+    desc = (f"every {CPU_EVERY}th set of the workload per step ({len(sample)} sets, {pts} points), "
+            f"one set per thread on {threads} host threads (each reference build is single-threaded)")
+    cfg["reference_sample"] = desc
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": cfg,
-            "cpu_baseline": {"value": value, "unit": "points/s", "cores": 1, "kind": "reference",
-                             "sample": f"{CPU_SAMPLE:.0e} uniform points per step, one thread "
-                                       "(the reference build is single-threaded)"},
+            "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads,
+                             "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+# ---- ours ----------------------------------------------------------------------------
+
+
+def traffic_per_attempt(kernel):
+    """DRAM bytes per insertion attempt of `kernel` from the committed ncu summary
+    (a line `<kernel> dram bytes per attempt: <number>`), or None."""
+    path = os.path.join(ROOT, "profiles", "traffic_per_attempt.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                m = re.search(rf"`{kernel}` dram bytes per attempt: ([0-9.]+)", line)
+                if m:
+                    return float(m.group(1))
+    except OSError:
+        return None
+    return None
+
+
+def plain_leg(torch, d3, x, offs, stream, out, sets_idx):
+    """The plain one-set-per-call path over the sets `sets_idx` (device-resident
+    slices of the batch input).  Returns per-set (points, ms)."""
+    handle = stream.cuda_stream
+    res = []
+    with torch.cuda.stream(stream):
+        for k in sets_idx[:8]:                         # warm-up calls
+            a, b = int(offs[k]), int(offs[k + 1])
+            d3.build_device(x[a:b], out=out, stream=handle)
+        torch.cuda.synchronize()
+        for k in sets_idx:
+            a, b = int(offs[k]), int(offs[k + 1])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            d3.build_device(x[a:b], out=out, stream=handle)
+            e1.record(stream)
+            e1.synchronize()
+            res.append((b - a, e0.elapsed_time(e1)))
+    return res
+
+
+def plain_1e7_leg(torch, d3, dev, stream, run_ref):
+    import oracle
+
+    host = d3.gen_uniform(PLAIN_N, PLAIN_SEED)
+    x = torch.from_numpy(host).to(dev)
+    out = torch.empty((8 * PLAIN_N + 64, 4), dtype=torch.int32, device=dev)
+    handle = stream.cuda_stream
+    ms = []
+    with torch.cuda.stream(stream):
+        d3.build_device(x, out=out, stream=handle)
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cells, _ = d3.build_device(x, out=out, stream=handle)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    ncells = int(cells.shape[0])
+    del x, out, cells
+    torch.cuda.empty_cache()
+    r = {"points": PLAIN_N, "ms": min(ms), "points_per_s": PLAIN_N / (min(ms) / 1000.0),
+         "tets": ncells}
+    if run_ref and oracle.ref_available():
+        sample = host[:REF_PLAIN_SAMPLE].copy()
+        nc = ctypes.c_int64(0)
+        t = oracle.ref().ref_build_time(sample.ctypes.data, sample.shape[0], ctypes.byref(nc))
+        r["reference_points_per_s_1thread"] = REF_PLAIN_SAMPLE / t
+        r["reference_sample"] = (f"first {REF_PLAIN_SAMPLE:.0e} of the same points, one thread "
+                                 f"({t:.2f} s; the reference build is single-threaded)")
+        r["gpu_over_reference"] = r["points_per_s"] / r["reference_points_per_s_1thread"]
+    return r
 
 
 def run_ours(args):
@@ -206,16 +349,26 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    n = args.n
-    host = d3.gen_uniform(n, SEED + rank)
-    x = torch.from_numpy(host).to(dev)
-    out = torch.empty((8 * n + 64, 4), dtype=torch.int32, device=dev)
+
+    t_gen = time.perf_counter()
+    sets = workload_sets(args.sets, rank)
+    t_gen = time.perf_counter() - t_gen
+    sizes = np.array([a.shape[0] for a in sets], dtype=np.int64)
+    offs = np.zeros(len(sets) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum(sizes)
+    n = int(offs[-1])
+    pinned = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    pin_np = pinned.numpy()
+    np.concatenate(sets, out=pin_np)
+    x = pinned.to(dev)
+    out = torch.empty((8 * n + 64 * len(sets), 4), dtype=torch.int32, device=dev)
     stream = torch.cuda.Stream(device=dev)
     handle = stream.cuda_stream
 
-    def step(timing=False, stats=None):
-        return d3.build_device(x, out=out, stream=handle, chunk=args.chunk, timing=timing,
-                               stats=stats)
+    def step(stats=None, timing=False):
+        if timing:
+            return _timed_batch(d3, x, offs, out, handle, args.chunk, stats)
+        return d3.build_batch_device(x, offs, out=out, stream=handle, chunk=args.chunk, stats=stats)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -232,8 +385,8 @@ def run_ours(args):
     ncells = 0
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
-            cells, nv = step()
-            ncells = cells.shape[0]
+            cells, co, nv = step()
+            ncells = int(cells.shape[0])
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop() if clocks else None
@@ -246,32 +399,68 @@ def run_ours(args):
     ms_max = float(t.item())
     value = world * n / (ms_max / 1000.0)
 
+    if args.profile_run:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                              "config": config(len(sets), n), "cells": ncells, "profile_run": True}))
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
     # ---- instrumented (untimed) step: per-kernel times and live counts ----
     stats = {}
     with torch.cuda.stream(stream):
-        step(timing=True, stats=stats)
+        step(stats=stats, timing=True)
     torch.cuda.synchronize()
     launches_per_step = count_launches(torch, lambda: step())
 
-    # ---- end to end through the host C ABI ----
-    pinned = torch.from_numpy(host).pin_memory()
-    pin_np = pinned.numpy()
-    d = d3.Delaunay()
-    d.build(pin_np)   # warm
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        d.build(pin_np)
-    t_e2e = (time.perf_counter() - t0) / args.steps
-    te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n / float(te.item())
-    off, inc = d.incident_csr()
-    d2h = 16 * (d.finite_cells().shape[0] + d.all_cells().shape[0]) + 8 * off.shape[0] + 4 * inc.shape[0]
+    # ---- end to end through the host C ABI d3g_build_batch ----
+    lib = d3.library()
+    opts = d3._Options()
+    lib.d3g_options_default(ctypes.byref(opts))
+    opts.chunk = int(args.chunk)
 
+    def e2e_call():
+        res = d3._BatchResult()
+        d3._check(lib.d3g_build_batch(pin_np.ctypes.data, offs.ctypes.data, len(sets),
+                                      ctypes.byref(opts), ctypes.byref(res)), "build_batch")
+        total = int(res.cell_offsets[len(sets)])
+        lib.d3g_batch_result_free(ctypes.byref(res))
+        return total
+
+    e2e_value, e2e_cells = None, 0
+    if not args.no_e2e:
+        e2e_call()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_cells = e2e_call()
+        t_e2e = (time.perf_counter() - t0) / args.steps
+        te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_value = world * n / float(te.item())
+
+    # ---- the plain one-set-per-call path on a sample of the same sets ----
+    plain = None
+    if not args.no_plain:
+        idx = list(range(0, len(sets), PLAIN_EVERY))
+        per = plain_leg(torch, d3, x, offs, stream, out, idx)
+        pts = sum(p for p, _ in per)
+        tot_ms = sum(m for _, m in per)
+        lat = [m for _, m in per]
+        plain = {"points_per_s": pts / (tot_ms / 1000.0),
+                 "sample": f"every {PLAIN_EVERY}th set ({len(idx)} sets, {pts} points), "
+                           "one d3g_build_device call per set, device-resident input",
+                 "latency_ms_p50": pct(lat, 50), "latency_ms_p99": pct(lat, 99),
+                 "latency_ms_max": max(lat)}
+        plain["batched_over_plain"] = (n / (ms / 1000.0)) / plain["points_per_s"]
+
+    line = None
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
@@ -287,40 +476,63 @@ def run_ours(args):
         bytes_kernel = {"k_cavity": 24 * (C + F) + 16 * C, "k_check": 8 * (C + F) + 16 * F,
                         "k_restar": 32 * C + 32 * F + 40 * F}[dom]
         achieved = (bytes_kernel / launches) / (kern[dom] / launches / 1000.0) / 1e9 if kern[dom] else 0.0
-        traffic = None
-        prof = os.path.join(ROOT, "profiles", "traffic_per_attempt.json")
-        if os.path.exists(prof):
-            try:
-                with open(prof) as f:
-                    per_attempt = json.load(f).get(dom)
-                if per_attempt:
-                    traffic = per_attempt * stats.get("attempts", 0) / launches
-            except (OSError, ValueError):
-                traffic = None
+        tpa = traffic_per_attempt(dom)
+        traffic = tpa * stats.get("attempts", 0) / launches if tpa else None
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload(n),
-            "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": 24 * n,
-                    "d2h_bytes_per_step": int(d2h)},
+            "data": "synthetic", "config": config(len(sets), n),
+            "tets_per_s": world * ncells / (ms_max / 1000.0),
+            "e2e": ({"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": 24 * n,
+                     "d2h_bytes_per_step": 16 * int(e2e_cells) + 16 * len(sets) + 8}
+                    if e2e_value else None),
+            "plain": plain,
+            "latency": {"batched_set_ms_p50": ms, "batched_set_ms_p99": ms,
+                        "note": "a batched set completes with its batch; plain = one call per set",
+                        "plain_set_ms_p50": plain["latency_ms_p50"] if plain else None,
+                        "plain_set_ms_p99": plain["latency_ms_p99"] if plain else None},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                          "traffic": traffic,
-                         "build_gbs": 132.0 * n / (ms_max / 1000.0) / 1e9,
-                         "build_frac": 132.0 * n / (ms_max / 1000.0) / 1e9 / hbm},
+                         "bytes_per_launch": bytes_kernel / launches,
+                         "ms_per_launch": kern[dom] / launches},
             "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
             "clocks": clk,
             "build_stats": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in stats.items()},
-            "cells": ncells,
+            "cells": ncells, "generate_s": round(t_gen, 2),
         }
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_leg()
+    if dist:
+        dist.barrier()
+    if rank == 0 and world == 1 and not args.no_plain:
+        line["plain_1e7"] = plain_1e7_leg(torch, d3, dev, stream, not args.no_cpu_baseline)
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_leg(sets)
+    if rank == 0:
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _timed_batch(d3, x, offs, out, handle, chunk, stats):
+    """One batched build with per-kernel event timing (slower; untimed)."""
+    import numpy as np
+
+    lib = d3.library()
+    nsets = offs.shape[0] - 1
+    co = np.zeros(nsets + 1, dtype=np.int64)
+    nv = np.zeros(nsets, dtype=np.int64)
+    opts = d3._Options()
+    lib.d3g_options_default(ctypes.byref(opts))
+    opts.chunk = int(chunk)
+    opts.timing = 1
+    st = d3.BuildStats()
+    d3._check(lib.d3g_build_batch_device(x.data_ptr(), offs.ctypes.data, nsets, ctypes.byref(opts),
+                                         out.data_ptr(), out.shape[0], co.ctypes.data, nv.ctypes.data,
+                                         ctypes.c_void_p(handle), ctypes.byref(st)), "build_batch_device")
+    stats.update(st.as_dict())
 
 
 def main():
