@@ -27,6 +27,11 @@ One JSON line (rank 0):
               the sets, one set per host thread.
   plain_1e7   the plain path on 1e7 uniform points and the reference's
               single-threaded build rate on 1e6 of them.
+  serving     the request server (d3g_server_*, continuous batching, admission
+              by device-memory budget) under Poisson arrivals swept over
+              several rates, request sizes log-uniform in [100, 1e6] points of
+              the same four distributions: points/s, requests/s and p50/p99
+              latency per rate.
 
 `--impl reference` times the reference's own CPU build on the same sample
 (rank 0 only; all host threads, one set per thread).
@@ -64,11 +69,15 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "predicates", "sort"],
+                    help="batched: the headline line; predicates / sort: the predicate and "
+                         "spatial-sort microbenchmarks, one line each")
     ap.add_argument("--sets", type=int, default=N_SETS)
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="warm-up and timed steps only (no other legs): the command profiled by ncu")
     return ap.parse_args()
@@ -330,6 +339,55 @@ def plain_1e7_leg(torch, d3, dev, stream, run_ref):
     return r
 
 
+SERVING_RATES = (25, 50, 100, 150)     # requests/s
+SERVING_SECONDS = 4.0
+SERVING_POOL = 160
+
+
+def serving_leg(torch, d3):
+    """Poisson request streams through d3.Server, one per rate."""
+    import numpy as np
+
+    pool = d3.mixed_workload(SERVING_POOL, lo=100, hi=1_000_000, seed=31, first_seed=7000)
+    pinned = []
+    for a in pool:
+        t = torch.empty(a.shape, dtype=torch.float64).pin_memory()
+        t.numpy()[:] = a
+        pinned.append(t.numpy())
+    sizes = np.array([a.shape[0] for a in pool])
+    out = []
+    with d3.Server(slots=4) as srv:
+        for t in [srv.submit(pinned[k]) for k in range(8)]:       # warm-up
+            srv.wait(t)
+        for rate in SERVING_RATES:
+            rng = np.random.default_rng(rate)
+            n_req = int(rate * SERVING_SECONDS)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+            picks = rng.integers(0, SERVING_POOL, n_req)
+            tickets = []
+            t0 = time.perf_counter()
+            for a, k in zip(arrivals, picks):
+                dt = t0 + a - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                tickets.append(srv.submit(pinned[k]))
+            res = [srv.wait(t) for t in tickets]
+            lat = [1000.0 * (r.t_done - r.t_submit) for r in res]
+            span = max(r.t_done for r in res) - min(r.t_submit for r in res)
+            pts = int(sizes[picks].sum())
+            out.append({"rate_req_per_s": rate, "requests": n_req, "points": pts,
+                        "points_per_s": pts / span, "requests_per_s": n_req / span,
+                        "latency_ms_p50": pct(lat, 50), "latency_ms_p99": pct(lat, 99),
+                        "mean_batch_sets": float(np.mean([r.batch_sets for r in res]))})
+        st = srv.stats()
+    return {"sweep": out, "slots": st["slots"], "hbm_budget_bytes": st["hbm_budget_bytes"],
+            "peak_bytes_in_use": st["peak_bytes_in_use"],
+            "workload": f"Poisson arrivals, {SERVING_SECONDS:.0f} s of arrivals per rate; each request "
+                        f"one of {SERVING_POOL} pre-generated sets (sizes log-uniform in [100, 1e6], "
+                        "uniform / 8-cluster / lattice / quantised sphere), pinned host memory; "
+                        "latency = submit to cells on the host"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -504,8 +562,11 @@ def run_ours(args):
         }
     if dist:
         dist.barrier()
-    if rank == 0 and world == 1 and not args.no_plain:
-        line["plain_1e7"] = plain_1e7_leg(torch, d3, dev, stream, not args.no_cpu_baseline)
+    if rank == 0 and world == 1:
+        if not args.no_plain:
+            line["plain_1e7"] = plain_1e7_leg(torch, d3, dev, stream, not args.no_cpu_baseline)
+        if not args.no_serving:
+            line["serving"] = serving_leg(torch, d3)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_leg(sets)
     if rank == 0:
@@ -535,10 +596,199 @@ def _timed_batch(d3, x, offs, out, handle, chunk, stats):
     stats.update(st.as_dict())
 
 
+# ---- microbenchmarks: predicates and spatial sort ------------------------------------
+
+PRED_POINTS = 10_000_000
+PRED_QUERIES = 100_000_000
+PRED_DEGENERATE = 0.10
+ORIENT3D_OPS, IN_SPHERE_OPS = 32, 111      # separate FP64 add/sub/mul of each filter
+
+
+def lattice_sphere_vectors(n2):
+    """Every integer vector (x, y, z) with x^2 + y^2 + z^2 = n2."""
+    import numpy as np
+
+    import math
+
+    r = math.isqrt(n2)
+    x, y = np.meshgrid(np.arange(-r, r + 1), np.arange(-r, r + 1), indexing="ij")
+    z2 = n2 - x * x - y * y
+    ok = z2 >= 0
+    x, y, z2 = x[ok], y[ok], z2[ok]
+    z = np.floor(np.sqrt(z2.astype(np.float64))).astype(np.int64)
+    z += (z + 1) * (z + 1) <= z2          # exact integer square root
+    z -= z * z > z2
+    hit = z * z == z2
+    x, y, z = x[hit], y[hit], z[hit]
+    v = np.concatenate([np.stack([x, y, z], 1), np.stack([x, y, -z], 1)[z > 0]])
+    return v
+
+
+def predicate_inputs(seed=2):
+    """Point table: 1e7 uniform in [-1,1]^3 (mt19937 seed 2), then groups of
+    points exactly degenerate by construction on a 2^-20 grid: 4 points on a
+    common lattice plane (orient3d) and 5 points on a common integer-lattice
+    sphere of squared radius 1221025 (= 1105^2, many representations) about a
+    grid-aligned centre (in_sphere).  Returns (points, n_uniform, plane_base,
+    n_plane_groups, sphere_base, n_sphere_groups)."""
+    import numpy as np
+
+    import del3d_b200 as d3
+
+    uni = d3.gen_uniform(PRED_POINTS, seed, -1.0, 1.0)
+    rng = np.random.default_rng(seed)
+    g4 = PRED_POINTS // 40
+    a = rng.integers(-2, 3, (g4, 1))
+    b = rng.integers(-2, 3, (g4, 1))
+    k = rng.integers(-(1 << 17), 1 << 17, (g4, 1))
+    i = rng.integers(-(1 << 17), 1 << 17, (g4, 4))
+    j = rng.integers(-(1 << 17), 1 << 17, (g4, 4))
+    plane = np.stack([i, j, k - a * i - b * j], axis=2).reshape(-1, 3) * 2.0 ** -20
+    vecs = lattice_sphere_vectors(1105 * 1105)
+    g5 = PRED_POINTS // 50
+    centre = rng.integers(-(1 << 19), 1 << 19, (g5, 1, 3))
+    pick = np.stack([rng.choice(len(vecs), 5, replace=False) for _ in range(64)])
+    sphere = (centre + vecs[pick[rng.integers(0, 64, g5)]]).reshape(-1, 3) * 2.0 ** -20
+    pts = np.ascontiguousarray(np.concatenate([uni, plane, sphere]))
+    return pts, PRED_POINTS, PRED_POINTS, g4, PRED_POINTS + 4 * g4, g5
+
+
+def predicate_queries(torch, dev, k, n_uniform, base, groups, n_q, seed):
+    """n_q index tuples of arity k on the device: 90% uniform random points,
+    10% one degenerate group each (rotated so the degenerate point order varies)."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    idx = torch.randint(0, n_uniform, (n_q, k), device=dev, dtype=torch.int32, generator=g)
+    n_deg = int(n_q * PRED_DEGENERATE)
+    rows = torch.randint(0, n_q, (n_deg,), device=dev, generator=g)
+    grp = torch.randint(0, groups, (n_deg, 1), device=dev, generator=g)
+    rot = torch.randint(0, k, (n_deg, 1), device=dev, generator=g)
+    col = (torch.arange(k, device=dev).view(1, k) + rot) % k
+    idx[rows] = (base + grp * k + col).to(torch.int32)
+    return idx.contiguous()
+
+
+def run_predicates(args):
+    import numpy as np
+    import torch
+
+    import del3d_b200 as d3
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    addmul, fma = d3.fp64_throughput(1 << 17, stream.cuda_stream)
+    pts_h, n_uni, pbase, g4, sbase, g5 = predicate_inputs()
+    pts = torch.from_numpy(pts_h).to(dev)
+    lib = d3.library()
+    res = {}
+    for kind, name, k, base, groups, ops in ((d3.ORIENT3D, "orient3d", 4, pbase, g4, ORIENT3D_OPS),
+                                             (d3.IN_SPHERE, "in_sphere", 5, sbase, g5, IN_SPHERE_OPS)):
+        idx = predicate_queries(torch, dev, k, n_uni, base, groups, PRED_QUERIES, 7 + k)
+        out = torch.empty(PRED_QUERIES, dtype=torch.int8, device=dev)
+        st = d3._PredStats()
+
+        def call():
+            d3._check(lib.d3g_predicates_device(pts.data_ptr(), pts.shape[0], idx.data_ptr(), PRED_QUERIES,
+                                                kind, out.data_ptr(), ctypes.c_void_p(stream.cuda_stream),
+                                                ctypes.byref(st)), name)
+
+        for _ in range(args.warmup):
+            call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        qps = PRED_QUERIES / (ms / 1000.0)
+        signs = torch.bincount((out.to(torch.int16) + 1).cpu(), minlength=3).tolist()
+        res[name] = {"queries": PRED_QUERIES, "ms": ms, "queries_per_s": qps,
+                     "exact_fraction": st.n_exact / PRED_QUERIES,
+                     "fp64_ops_per_query": ops, "fp64_ops_per_s": qps * ops,
+                     "fp64_frac_of_measured_addmul_peak": qps * ops / addmul,
+                     "signs_neg_zero_pos": signs}
+        del idx, out
+    line = {"metric": "predicate queries/s (filter + exact stage + perturbation)",
+            "value": 2 * PRED_QUERIES / sum(r["ms"] / 1000.0 for r in res.values()),
+            "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"1e8 orient3d + 1e8 in_sphere over a table of 1e7 points uniform in "
+                                   f"[-1,1]^3 plus exactly degenerate groups on a 2^-20 grid "
+                                   f"({PRED_DEGENERATE:.0%} of queries): lattice planes (orient3d), "
+                                   f"integer-lattice spheres (in_sphere)",
+                       "l2": "index arrays 1.6-2 GB per kind (larger than L2)"},
+            "fp64_peak": {"addmul_ops_per_s": addmul, "dfma_per_s": fma,
+                          "note": "measured here by d3g_microbench_fp64"},
+            "predicates": res}
+    print(json.dumps(line))
+    return 0
+
+
+SORT_N = 10_000_000
+
+
+def run_sort(args):
+    import torch
+
+    import del3d_b200 as d3
+    import oracle
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    host = d3.gen_uniform(SORT_N, 3)
+    x = torch.from_numpy(host).to(dev)
+    order = torch.empty(SORT_N, dtype=torch.int32, device=dev)
+    lib = d3.library()
+
+    def call():
+        d3._check(lib.d3g_spatial_sort_device(x.data_ptr(), SORT_N, order.data_ptr(),
+                                              ctypes.c_void_p(stream.cuda_stream)), "spatial_sort")
+
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
+    gbs = 28.0 * SORT_N / (ms / 1000.0) / 1e9
+    line = {"metric": "spatial sort points/s (bit-exact reference order)", "value": SORT_N / (ms / 1000.0),
+            "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "1e7 points uniform in [0,1)^3 (mt19937 seed 3)"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "peak_kind": peak_kind, "bytes_per_point": 28}}
+    if oracle.ref_available() and not args.no_cpu_baseline:
+        import numpy as np
+
+        o = np.zeros(SORT_N, dtype=np.int32)
+        t0 = time.perf_counter()
+        oracle.ref().ref_spatial_sort(host.ctypes.data, SORT_N, o.ctypes.data)
+        t = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": SORT_N / t, "unit": "points/s", "cores": 1, "kind": "reference",
+                                "sample": f"the whole 1e7 points, one thread ({t:.2f} s)"}
+        line["order_equals_reference"] = bool(np.array_equal(o, order.cpu().numpy()))
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "predicates":
+        return run_predicates(args)
+    if args.workload == "sort":
+        return run_sort(args)
     return run_ours(args)
 
 

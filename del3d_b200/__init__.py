@@ -31,7 +31,8 @@ import numpy as np
 __all__ = [
     "Del3dError", "Delaunay", "Point3", "orient3d", "in_sphere", "in_sphere_unperturbed",
     "orient2d", "coplanar_orientation", "coplanar_in_circle", "coplanar_in_circle_unperturbed",
-    "collinear", "spatial_sort", "library", "LIB_PATH", "predicate_stats",
+    "collinear", "spatial_sort", "library", "LIB_PATH", "predicate_stats", "circumcenters",
+    "circumcenter", "circumcenter_lazy", "Server", "Request", "pool_usage",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -61,7 +62,8 @@ class BuildStats(ctypes.Structure):
                 ("boundary_facets", _I64), ("ms_order", ctypes.c_double),
                 ("ms_rounds", ctypes.c_double), ("ms_output", ctypes.c_double),
                 ("ms_cavity", ctypes.c_double), ("ms_check", ctypes.c_double),
-                ("ms_restar", ctypes.c_double), ("launches_cavity", _I64)]
+                ("ms_restar", ctypes.c_double), ("launches_cavity", _I64),
+                ("walk_steps", _I64), ("bfs_steps", _I64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -85,6 +87,26 @@ class _BatchResult(ctypes.Structure):
     _fields_ = [("n_sets", _I32), ("cell_offsets", ctypes.POINTER(_I64)),
                 ("cells", ctypes.POINTER(_I32)), ("n_vertices", ctypes.POINTER(_I64)),
                 ("device_ms", ctypes.c_double), ("stats", BuildStats)]
+
+
+class _ServerOptions(ctypes.Structure):
+    _fields_ = [("slots", _I32), ("hbm_budget_bytes", _I64), ("max_batch_sets", _I32),
+                ("max_batch_points", _I64), ("device", _I32)]
+
+
+class _RequestResult(ctypes.Structure):
+    _fields_ = [("status", _I32), ("n_points", _I64), ("n_vertices", _I64), ("n_cells", _I64),
+                ("cells", ctypes.POINTER(_I32)), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double), ("batch_sets", _I32)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", _I64), ("completed", _I64), ("queued", _I64), ("batches", _I64),
+                ("batched_requests", _I64), ("bytes_in_use", _I64), ("peak_bytes_in_use", _I64),
+                ("hbm_budget_bytes", _I64), ("peak_in_flight_requests", _I64), ("slots", _I32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class _PredStats(ctypes.Structure):
@@ -129,6 +151,28 @@ def library() -> ctypes.CDLL:
     lib.d3g_build_batch_device.argtypes = [_P, _P, _I32, ctypes.POINTER(_Options), _P, _I64, _P, _P, _P,
                                            ctypes.POINTER(BuildStats)]
     lib.d3g_build_batch_device.restype = _INT
+    lib.d3g_circumcenters.argtypes = [_P, _I64, _P, _I64, _INT, _P, ctypes.POINTER(_PredStats)]
+    lib.d3g_circumcenters.restype = _INT
+    lib.d3g_circumcenters_device.argtypes = [_P, _I64, _P, _I64, _INT, _P, _P, ctypes.POINTER(_PredStats)]
+    lib.d3g_circumcenters_device.restype = _INT
+    lib.d3g_server_options_default.argtypes = [ctypes.POINTER(_ServerOptions)]
+    lib.d3g_server_options_default.restype = None
+    lib.d3g_server_create.argtypes = [ctypes.POINTER(_ServerOptions), ctypes.POINTER(_P)]
+    lib.d3g_server_create.restype = _INT
+    lib.d3g_server_submit.argtypes = [_P, _P, _I64, ctypes.POINTER(_I64)]
+    lib.d3g_server_submit.restype = _INT
+    lib.d3g_server_wait.argtypes = [_P, _I64, ctypes.c_double, ctypes.POINTER(_RequestResult)]
+    lib.d3g_server_wait.restype = _INT
+    lib.d3g_request_result_free.argtypes = [ctypes.POINTER(_RequestResult)]
+    lib.d3g_request_result_free.restype = None
+    lib.d3g_server_get_stats.argtypes = [_P, ctypes.POINTER(_ServerStats)]
+    lib.d3g_server_get_stats.restype = _INT
+    lib.d3g_server_destroy.argtypes = [_P]
+    lib.d3g_server_destroy.restype = _INT
+    lib.d3g_microbench_fp64.argtypes = [_I64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]
+    lib.d3g_microbench_fp64.restype = _INT
+    lib.d3g_pool_usage.argtypes = [ctypes.POINTER(_I64), ctypes.POINTER(_I64), _INT]
+    lib.d3g_pool_usage.restype = _INT
     lib.d3g_gen_uniform.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, _P]
     lib.d3g_gen_sphere.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, _I32, _P]
     lib.d3g_gen_clusters.argtypes = [_I64, ctypes.c_uint32, _I32, ctypes.c_double, _P]
@@ -260,6 +304,34 @@ def orient2d(six) -> np.ndarray:
     out = np.zeros(a.shape[0], dtype=np.int8)
     _check(lib.d3g_orient2d(_ptr(a), a.shape[0], _ptr(out)), "orient2d")
     return out
+
+
+def circumcenters(points, tets, lazy: bool = False) -> np.ndarray:
+    """Circumcentre of every tet (rows of 4 indices into `points`), (n, 3)
+    float64: del3d::circumcenter, or del3d::circumcenter_lazy with lazy=True
+    (reference delaunay.h:29, :48).  A coplanar tet gives its first vertex."""
+    global _last_pred_stats
+    lib = library()
+    pts = _points(points)
+    t = np.ascontiguousarray(tets, dtype=np.int32).reshape(-1, 4)
+    out = np.zeros((t.shape[0], 3), dtype=np.float64)
+    st = _PredStats()
+    _check(lib.d3g_circumcenters(_ptr(pts), pts.shape[0], _ptr(t), t.shape[0], int(lazy), _ptr(out),
+                                 ctypes.byref(st)), "circumcenters")
+    _last_pred_stats = (st.n_queries, st.n_exact)
+    return out
+
+
+def circumcenter(p0, p1, p2, p3) -> Point3:
+    """del3d::circumcenter of one tetrahedron (reference delaunay.h:29)."""
+    c = circumcenters([tuple(p0), tuple(p1), tuple(p2), tuple(p3)], [[0, 1, 2, 3]])[0]
+    return Point3(*c)
+
+
+def circumcenter_lazy(p, q, r, s) -> Point3:
+    """del3d::circumcenter_lazy of one tetrahedron (reference delaunay.h:48)."""
+    c = circumcenters([tuple(p), tuple(q), tuple(r), tuple(s)], [[0, 1, 2, 3]], lazy=True)[0]
+    return Point3(*c)
 
 
 def spatial_sort(points, order: Optional[List[int]] = None) -> np.ndarray:
@@ -435,6 +507,114 @@ def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk
     if stats is not None:
         stats.update(st.as_dict())
     return out[: int(co[-1])], co, nv
+
+
+# ---- serving --------------------------------------------------------------------
+
+
+NOT_READY = 11
+
+
+class Request:
+    """A completed request: its finite cells (canonical order, indices into the
+    request's points), vertex count and timestamps (seconds since the server
+    started)."""
+
+    __slots__ = ("cells", "n_vertices", "t_submit", "t_admit", "t_done", "batch_sets")
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
+
+
+class Server:
+    """Continuous-batching request server on one GPU (d3g_server_*).
+
+    ``submit(points)`` queues a triangulation request and returns a ticket;
+    ``wait(ticket)`` returns its :class:`Request`.  Free slots (each a worker
+    with its own CUDA stream) take the pending requests in arrival order while
+    they fit the batch limits and the device-memory budget, so requests that
+    arrive while others run are admitted as slots and memory free up.  Each
+    request's cells equal ``Delaunay().build(points).finite_cells()``.
+    Thread-safe; use as a context manager or call :meth:`close`."""
+
+    def __init__(self, slots: int = 4, hbm_budget_bytes: int = 0, max_batch_sets: int = 1024,
+                 max_batch_points: int = 8 << 20, device: int = -1):
+        lib = library()
+        o = _ServerOptions()
+        lib.d3g_server_options_default(ctypes.byref(o))
+        o.slots, o.hbm_budget_bytes = int(slots), int(hbm_budget_bytes)
+        o.max_batch_sets, o.max_batch_points, o.device = int(max_batch_sets), int(max_batch_points), int(device)
+        h = _P()
+        _check(lib.d3g_server_create(ctypes.byref(o), ctypes.byref(h)), "server_create")
+        self._h = h
+        self._keep = {}          # ticket -> input array (borrowed by the server until done)
+
+    def submit(self, points) -> int:
+        pts = _points(points)
+        t = _I64(0)
+        _check(library().d3g_server_submit(self._h, _ptr(pts) if pts.shape[0] else None, pts.shape[0],
+                                           ctypes.byref(t)), "server_submit")
+        self._keep[t.value] = pts
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = -1.0) -> Request:
+        lib = library()
+        res = _RequestResult()
+        st = lib.d3g_server_wait(self._h, int(ticket), float(timeout), ctypes.byref(res))
+        if st == NOT_READY:
+            raise TimeoutError(f"request {ticket} not complete within {timeout} s")
+        self._keep.pop(int(ticket), None)
+        try:
+            _check(st, "server_wait")
+            r = Request()
+            nc = res.n_cells
+            r.cells = (np.ctypeslib.as_array(res.cells, shape=(nc * 4,)).reshape(nc, 4).copy()
+                       if nc else np.zeros((0, 4), dtype=np.int32))
+            r.n_vertices = int(res.n_vertices)
+            r.t_submit, r.t_admit, r.t_done = res.t_submit, res.t_admit, res.t_done
+            r.batch_sets = int(res.batch_sets)
+            return r
+        finally:
+            lib.d3g_request_result_free(ctypes.byref(res))
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(library().d3g_server_get_stats(self._h, ctypes.byref(st)), "server_stats")
+        return st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().d3g_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def fp64_throughput(iters: int = 1 << 16, stream: int = 0):
+    """(separate DADD/DMUL operations/s, DFMA/s) of the current device."""
+    a, f = ctypes.c_double(0), ctypes.c_double(0)
+    _check(library().d3g_microbench_fp64(int(iters), ctypes.byref(a), ctypes.byref(f), _P(stream)),
+           "microbench_fp64")
+    return a.value, f.value
+
+
+def pool_usage(reset_high: bool = False):
+    """(bytes in use, high-water mark) of the current device's stream-ordered pool."""
+    u, h = _I64(0), _I64(0)
+    _check(library().d3g_pool_usage(ctypes.byref(u), ctypes.byref(h), int(reset_high)), "pool_usage")
+    return u.value, h.value
 
 
 # ---- synthetic inputs -------------------------------------------------------------

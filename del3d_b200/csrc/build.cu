@@ -29,6 +29,7 @@
 //
 // The output is canonicalised (even rotation, lexicographic sort), so it is
 // identical across runs whatever order the rounds happened to take.
+#include "build_api.cuh"
 #include "device_util.cuh"
 
 #include <algorithm>
@@ -121,6 +122,8 @@ struct Round {
     unsigned long long* sums; // [0] region tets, [1] boundary facets of the winners
     unsigned long long* totals; // [0] winners, [1] attempts, [2] rounds with work,
                                 // [3] parked workers, [4] stalled round seen, [5] active
+    unsigned long long* steps;  // timing runs only (else null): [0] walk steps,
+                                // [1] breadth-first steps, over all attempts
     uint32_t* status;
 };
 
@@ -189,7 +192,7 @@ constexpr unsigned kFull = 0xffffffffu;
 /// first negative one in a pseudo-random cyclic order is crossed (never the
 /// facet just crossed).  Every lane returns the same tet.
 __device__ int walk_w(int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
-                      uint32_t* st, int lane) {
+                      uint32_t* st, int lane, int* nsteps) {
     int4 tv = T.tv[t];
     {
         const int ip = inf_pos(tv);
@@ -210,6 +213,7 @@ __device__ int walk_w(int t, const Pt& p, int pid, const Tables& T, const double
             neg = orient_replaced(q, lane, p, st) < 0;
         }
         const unsigned m = __ballot_sync(kFull, neg) & 0xFu;
+        *nsteps = step + 1;
         if (m == 0) return t;
         const unsigned rot = ((m >> s0) | (m << (4 - s0))) & 0xFu;
         const int i = (s0 + __ffs(int(rot)) - 1) & 3;
@@ -263,7 +267,9 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
     }
     const Pt p = vpt(vx, v);
     const int sv = W.last[w] >= 0 ? W.last[w] : W.guide[w];
-    const int seed = walk_w(T.vert_tet[sv], p, v, T, vx, R.status, lane);
+    int wsteps = 0;
+    const int seed = walk_w(T.vert_tet[sv], p, v, T, vx, R.status, lane, &wsteps);
+    if (R.steps && lane == 0) atomicAdd(R.steps, (unsigned long long)wsteps);
     if (seed < 0) {
         if (lane == 0) W.state[w] = WS_FAIL;
         return;
@@ -286,6 +292,7 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
     const unsigned lt = (1u << lane) - 1u;
     int ncav = 1, nfac = 0, head = 0;
     while (head < ncav) {
+        if (R.steps && lane == 0) atomicAdd(R.steps + 1, 1ull);
         const int nproc = min(ncav - head, 8);
         const bool valid = (lane >> 2) < nproc;
         const int i = lane & 3;
@@ -913,28 +920,6 @@ __global__ void k_widen(const int32_t* __restrict__ a, int64_t m, int64_t* __res
 
 }  // namespace
 
-/// Device-resident result of one build of one or more sets.
-struct DeviceResult {
-    DevBuf<int4> cells;          // finite cells of every set, set by set, canonical order
-    DevBuf<int4> all;            // single set only: all cells
-    DevBuf<int64_t> inc_off;     // single set only: incident CSR
-    DevBuf<int32_t> inc;
-    int64_t n_cells = 0, n_all = 0, n_vertices = 0, n_inc = 0;
-    std::vector<int64_t> cell_off;   // per set: [cell_off[s], cell_off[s+1]) of `cells`
-    std::vector<int64_t> set_nv;     // per set: distinct points
-    d3g_build_stats stats{};
-    void reset() {
-        cells.release();
-        all.release();
-        inc_off.release();
-        inc.release();
-        n_cells = n_all = n_vertices = n_inc = 0;
-        cell_off.clear();
-        set_nv.clear();
-        stats = d3g_build_stats{};
-    }
-};
-
 namespace {
 
 __global__ void k_voff(const int64_t* __restrict__ off, int nsets, const int32_t* __restrict__ vid, bool dups,
@@ -1295,9 +1280,11 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     D3G_TRY(wsv.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(wsn.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(counters.alloc(4, s));
-    DevBuf<unsigned long long> sums, totals;
+    DevBuf<unsigned long long> sums, totals, steps;
     DevBuf<unsigned> dround;
     D3G_TRY(sums.alloc(2, s));
+    D3G_TRY(steps.alloc(2, s));
+    D3G_CUDA(cudaMemsetAsync(steps.p, 0, 2 * sizeof(unsigned long long), s));
     D3G_TRY(totals.alloc(6, s));
     D3G_TRY(dround.alloc(1, s));
     D3G_CUDA(cudaMemsetAsync(sums.p, 0, 2 * sizeof(unsigned long long), s));
@@ -1327,6 +1314,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     Rd.counters = counters.p;
     Rd.sums = sums.p;
     Rd.totals = totals.p;
+    Rd.steps = opt.timing ? steps.p : nullptr;
     Rd.round = dround.p;
     Rd.status = status.p;
     const int max_rounds = opt.max_rounds > 0 ? opt.max_rounds : (1 << 20);
@@ -1545,14 +1533,17 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         }
     }
     {
-        unsigned long long hs2[2] = {0, 0}, ht[6];
+        unsigned long long hs2[2] = {0, 0}, ht[6], hst[2] = {0, 0};
         D3G_CUDA(cudaMemcpyAsync(hs2, sums.p, sizeof hs2, cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaMemcpyAsync(hst, steps.p, sizeof hst, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaMemcpyAsync(ht, totals.p, sizeof ht, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaStreamSynchronize(s));
         R.stats.region_tets = int64_t(hs2[0]);
         R.stats.boundary_facets = int64_t(hs2[1]);
         R.stats.rounds = int(ht[2]);
         R.stats.attempts = int64_t(ht[1]);
+        R.stats.walk_steps = int64_t(hst[0]);
+        R.stats.bfs_steps = int64_t(hst[1]);
     }
     // Release round scratch before the output stage.
     wcav.release();

@@ -87,6 +87,7 @@ const char* d3g_status_string(int status) {
         case D3G_ERR_CUDA: return "CUDA error";
         case D3G_ERR_INTERNAL: return "internal error";
         case D3G_ERR_NO_DEVICE: return "no CUDA device";
+        case D3G_ERR_NOT_READY: return "not complete yet";
         default: return "unknown status";
     }
 }

@@ -44,7 +44,8 @@ typedef enum d3g_status {
     D3G_ERR_ROUND_LIMIT = 7,      /* insertion rounds hit their limit            */
     D3G_ERR_CUDA = 8,             /* a CUDA runtime call failed                  */
     D3G_ERR_INTERNAL = 9,         /* an internal invariant did not hold          */
-    D3G_ERR_NO_DEVICE = 10        /* no CUDA device could be used                */
+    D3G_ERR_NO_DEVICE = 10,       /* no CUDA device could be used                */
+    D3G_ERR_NOT_READY = 11        /* d3g_server_wait: not complete within timeout */
 } d3g_status;
 
 /* Human-readable name of a status; never NULL. */
@@ -114,6 +115,24 @@ int d3g_predicates_noalloc_device(const double* d_pts, int64_t n_pts, const int3
 /* del3d::orient2d(px,py,qx,qy,rx,ry) over `six` (6 doubles per query); host pointers. */
 int d3g_orient2d(const double* six, int64_t n_queries, int8_t* sign_out);
 
+/* ---- circumcentres ---------------------------------------------------------
+ * lazy = 0: del3d::circumcenter (reference include/del3d/delaunay.h:29,
+ * src/triangulation.cpp:805-852); lazy = 1: del3d::circumcenter_lazy
+ * (delaunay.h:48, triangulation.cpp:873-930).  `tets`: 4 indices into `pts` per
+ * tet; `out`: x y z per tet.  A coplanar tet gives its first vertex, as in the
+ * reference.  The lazy form is the reference's value bit for bit where its
+ * interval pass decides a coordinate; a coordinate that needs the exact
+ * fallback, and every coordinate of the exact form, is the reference's value
+ * within 4 ulp of the quotient nx/den plus 1 ulp of the result (bit-identical
+ * whenever the reference's expansion sum is the nearest double).
+ * stats->n_exact: tets that needed exact arithmetic (all of them for lazy = 0).
+ * Returns D3G_ERR_INVALID_INPUT for an index out of range. */
+int d3g_circumcenters(const double* pts, int64_t n_pts, const int32_t* tets, int64_t n_tets, int lazy,
+                      double* out, d3g_predicate_stats* stats);
+/* Device pointers on `stream`; synchronises `stream`. */
+int d3g_circumcenters_device(const double* d_pts, int64_t n_pts, const int32_t* d_tets, int64_t n_tets,
+                             int lazy, double* d_out, void* stream, d3g_predicate_stats* stats);
+
 /* ---- spatial sort ----------------------------------------------------------
  * The reference insertion order (rand48 shuffle, multiscale split, Hilbert
  * median splits), bit for bit: order[k] = index of the k-th point. */
@@ -153,6 +172,8 @@ typedef struct d3g_build_stats {
     /* with d3g_options.timing: device time of each insertion kernel, summed */
     double ms_cavity, ms_check, ms_restar;
     int64_t launches_cavity;
+    int64_t walk_steps;      /* with timing: point-location steps over all attempts  */
+    int64_t bfs_steps;       /* with timing: conflict-region growth steps (8 tets each) */
 } d3g_build_stats;
 
 typedef struct d3g_result {
@@ -223,6 +244,74 @@ void d3g_gen_sphere(int64_t n, uint32_t seed, double r, int32_t q, double* xyz);
 void d3g_gen_clusters(int64_t n, uint32_t seed, int32_t k, double sigma, double* xyz);
 /* The first n points of the integer lattice of side ceil(n^(1/3)), lexicographic. */
 void d3g_gen_lattice(int64_t n, double* xyz);
+
+/* ---- serving ----------------------------------------------------------------
+ * A request server on one GPU with continuous batching.  No counterpart in the
+ * reference (one single-threaded build per call); each request's cells are
+ * exactly what d3g_build returns for its points alone.
+ *   - `slots` worker threads, each with its own CUDA stream: up to `slots`
+ *     batches run on the device at once.
+ *   - A free slot takes pending requests in arrival order while they fit: at
+ *     most max_batch_sets requests and max_batch_points points per batch, and
+ *     the estimated device memory of all in-flight batches within
+ *     hbm_budget_bytes (a request larger than the budget runs alone once
+ *     nothing else is in flight).  Requests arriving while batches run are
+ *     admitted as soon as a slot and memory free up.
+ *   - Points and tets stay on the device for the whole build; each request's
+ *     cells are copied to a host buffer of its own.
+ * Thread-safe: submit and wait may be called from any threads. */
+typedef struct d3g_server d3g_server;
+
+typedef struct d3g_server_options {
+    int32_t slots;             /* batches in flight at once (default 4)                       */
+    int64_t hbm_budget_bytes;  /* device memory for in-flight batches; 0 = half the free
+                                  memory at creation (default 0)                             */
+    int32_t max_batch_sets;    /* requests per batch (default 1024)                           */
+    int64_t max_batch_points;  /* points per batch (default 8 Mi)                             */
+    int32_t device;            /* CUDA device; -1 = the current one (default -1)              */
+} d3g_server_options;
+
+typedef struct d3g_request_result {
+    int32_t status;            /* D3G_OK or the build's status for this request              */
+    int64_t n_points, n_vertices, n_cells;
+    int32_t* cells;            /* n_cells x 4 int32, canonical order, indices into the
+                                  request's points; free with d3g_request_result_free        */
+    double t_submit, t_admit, t_done;  /* seconds since the server was created              */
+    int32_t batch_sets;        /* requests in the batch it was built in                      */
+} d3g_request_result;
+
+typedef struct d3g_server_stats {
+    int64_t submitted, completed, queued, batches, batched_requests;
+    int64_t bytes_in_use, peak_bytes_in_use, hbm_budget_bytes;  /* admission estimates */
+    int64_t peak_in_flight_requests;
+    int32_t slots;
+} d3g_server_stats;
+
+void d3g_server_options_default(d3g_server_options* o);
+int d3g_server_create(const d3g_server_options* o, d3g_server** out);
+/* Queues a request of n points (3 doubles each, host memory; pinned memory
+ * copies fastest).  `xyz` is borrowed until the request completes. */
+int d3g_server_submit(d3g_server* s, const double* xyz, int64_t n, int64_t* ticket);
+/* Waits for request `ticket` (timeout_s < 0: no limit) and hands over its
+ * result, once; returns the request's status, or D3G_ERR_NOT_READY on timeout
+ * (the ticket stays valid). */
+int d3g_server_wait(d3g_server* s, int64_t ticket, double timeout_s, d3g_request_result* out);
+void d3g_request_result_free(d3g_request_result* r);
+int d3g_server_get_stats(d3g_server* s, d3g_server_stats* out);
+/* Completes every queued and in-flight request, then frees the server and any
+ * results not collected. */
+int d3g_server_destroy(d3g_server* s);
+
+/* The current device's stream-ordered pool: bytes in use and the high-water
+ * mark since the last reset (reset_high != 0 resets it). */
+int d3g_pool_usage(int64_t* used, int64_t* used_high, int reset_high);
+
+/* ---- measurement aid ------------------------------------------------------------
+ * FP64 throughput of the current device with the filters' arithmetic: separate
+ * DADD/DMUL operations per second (the filters are built without contraction)
+ * and, for comparison, DFMA instructions per second; `iters` steps of 8
+ * independent chains per thread.  No counterpart in the reference. */
+int d3g_microbench_fp64(int64_t iters, double* addmul_ops_per_s, double* fma_per_s, void* stream);
 
 #ifdef __cplusplus
 }

@@ -182,6 +182,17 @@ def orc_build(pts: np.ndarray) -> dict:
         lib.orc_build_free(h)
 
 
+def ref_circumcenters(pts: np.ndarray, tets: np.ndarray, lazy: bool = False) -> np.ndarray:
+    """The reference's del3d::circumcenter (or circumcenter_lazy) per tet
+    (src/triangulation.cpp:805-930), (n, 3) float64."""
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    t = np.ascontiguousarray(tets, dtype=np.int32).reshape(-1, 4)
+    out = np.zeros((t.shape[0], 3), dtype=np.float64)
+    if t.shape[0]:
+        ref().ref_circumcenter(_ptr(pts), _ptr(t), t.shape[0], int(lazy), _ptr(out))
+    return out
+
+
 def ref_build(pts: np.ndarray) -> dict:
     """The reference build's outputs, in the reference's own (allocation) order."""
     pts = np.ascontiguousarray(pts, dtype=np.float64)
