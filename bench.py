@@ -69,9 +69,14 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "predicates", "sort"],
-                    help="batched: the headline line; predicates / sort: the predicate and "
+    ap.add_argument("--workload", default="batched", choices=["batched", "plain", "predicates", "sort"],
+                    help="batched: the headline line; plain: one single-set build per step "
+                         "(--n uniform points); predicates / sort: the predicate and "
                          "spatial-sort microbenchmarks, one line each")
+    ap.add_argument("--n", type=int, default=PLAIN_N, help="points of the plain workload")
+    ap.add_argument("--timing", action="store_true",
+                    help="plain workload: launch each round's kernels separately with event "
+                         "timing (the form the ncu launch list captures)")
     ap.add_argument("--sets", type=int, default=N_SETS)
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -727,6 +732,39 @@ def run_predicates(args):
     return 0
 
 
+def run_plain(args):
+    """One plain single-set build of --n uniform points per step (mt19937 seed 6)."""
+    import torch
+
+    import del3d_b200 as d3
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    x = torch.from_numpy(d3.gen_uniform(args.n, PLAIN_SEED)).to(dev)
+    out = torch.empty((8 * args.n + 64, 4), dtype=torch.int32, device=dev)
+    stats = {}
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            d3.build_device(x, out=out, stream=stream.cuda_stream, timing=args.timing)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            cells, _ = d3.build_device(x, out=out, stream=stream.cuda_stream, timing=args.timing,
+                                       stats=stats)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"metric": "plain single-set build points/s", "value": args.n / (ms / 1000.0),
+                      "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": ms, "timing": bool(args.timing), "cells": int(cells.shape[0]),
+                      "config": {"workload": f"{args.n} points uniform in [0,1)^3 (mt19937 seed {PLAIN_SEED})"},
+                      "build_stats": {k: (round(v, 3) if isinstance(v, float) else v)
+                                      for k, v in stats.items()}}))
+    return 0
+
+
 SORT_N = 10_000_000
 
 
@@ -789,6 +827,8 @@ def main():
         return run_predicates(args)
     if args.workload == "sort":
         return run_sort(args)
+    if args.workload == "plain":
+        return run_plain(args)
     return run_ours(args)
 
 

@@ -80,7 +80,8 @@ class _Result(ctypes.Structure):
 
 class _Options(ctypes.Structure):
     _fields_ = [("want_all_cells", _I32), ("want_incident", _I32), ("chunk", _I32),
-                ("max_rounds", _I32), ("timing", _I32), ("alpha_small", _I32), ("split", _I32)]
+                ("max_rounds", _I32), ("timing", _I32), ("alpha_small", _I32), ("split", _I32),
+                ("lanes", _I32), ("schedule", _I32)]
 
 
 class _BatchResult(ctypes.Structure):
@@ -386,7 +387,10 @@ class Delaunay:
             self._all = (np.ctypeslib.as_array(res.all_cells, shape=(na * 4,)).reshape(na, 4).copy()
                          if na else np.zeros((0, 4), dtype=np.int32))
             n = pts.shape[0]
-            self._inc_off = np.ctypeslib.as_array(res.incident_offsets, shape=(n + 1,)).copy()
+            if res.incident_offsets:
+                self._inc_off = np.ctypeslib.as_array(res.incident_offsets, shape=(n + 1,)).copy()
+            else:                                   # incident lists not asked for
+                self._inc_off = np.zeros(n + 1, dtype=np.int64)
             ninc = int(self._inc_off[-1])
             self._inc = (np.ctypeslib.as_array(res.incident, shape=(ninc,)).copy()
                          if ninc else np.zeros(0, dtype=np.int32))
@@ -419,7 +423,8 @@ class Delaunay:
 
 
 def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: bool = False,
-                 stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0):
+                 stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0, lanes: int = 0,
+                 schedule: int = 0):
     """Builds from a device-resident torch tensor (n, 3) float64 on `stream`
     (a raw cudaStream_t handle; 0 = default) and returns the canonical finite
     cells as a device int32 tensor view (n_cells, 4) and the vertex count.
@@ -439,6 +444,8 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: 
     opts.timing = int(timing)
     opts.alpha_small = int(alpha_small)
     opts.split = int(split)
+    opts.lanes = int(lanes)
+    opts.schedule = int(schedule)
     st = BuildStats()
     _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), out.shape[0],
                                 ctypes.byref(nc), ctypes.byref(nv), _P(stream), ctypes.byref(st)),
@@ -480,7 +487,8 @@ def build_batch(sets, chunk: int = 0, stats: Optional[dict] = None):
 
 
 def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk: int = 0,
-                       stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0):
+                       stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0,
+                       lanes: int = 0, schedule: int = 0):
     """Device-resident form of build_batch: `points_dev` (n, 3) float64 CUDA
     tensor holding the sets back to back, `set_offsets` (n_sets + 1) host
     int64.  Returns the device cells tensor (all sets), the cell offsets per
@@ -500,6 +508,8 @@ def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk
     opts.chunk = int(chunk)
     opts.alpha_small = int(alpha_small)
     opts.split = int(split)
+    opts.lanes = int(lanes)
+    opts.schedule = int(schedule)
     st = BuildStats()
     _check(lib.d3g_build_batch_device(x.data_ptr(), _ptr(offs), nsets, ctypes.byref(opts), out.data_ptr(),
                                       out.shape[0], _ptr(co), _ptr(nv), _P(stream), ctypes.byref(st)),

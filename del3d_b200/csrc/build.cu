@@ -30,9 +30,12 @@
 // The output is canonicalised (even rotation, lexicographic sort), so it is
 // identical across runs whatever order the rounds happened to take.
 #include "build_api.cuh"
+
+#include <cuda/atomic>
 #include "device_util.cuh"
 
 #include <algorithm>
+#include <numeric>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -186,48 +189,6 @@ __device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __
 
 constexpr unsigned kFull = 0xffffffffu;
 
-/// Visibility walk from tet t to a tet in conflict with p: the finite tet
-/// containing p, or the infinite tet beyond the hull facet the walk crosses.
-/// Warp-cooperative: the four facet tests of a step run on lanes 0-3 and the
-/// first negative one in a pseudo-random cyclic order is crossed (never the
-/// facet just crossed).  Every lane returns the same tet.
-__device__ int walk_w(int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
-                      uint32_t* st, int lane, int* nsteps) {
-    int4 tv = T.tv[t];
-    {
-        const int ip = inf_pos(tv);
-        if (ip >= 0) {
-            t = at(T.tn[t], ip) >> 2;
-            tv = T.tv[t];
-        }
-    }
-    int prev = -1;
-    uint32_t h = uint32_t(pid) * 2654435761u + 12345u;
-    for (int step = 0; step < kWalkLimit; ++step) {
-        const int4 tn = T.tn[t];
-        h = h * 1664525u + 1013904223u;
-        const int s0 = int(h >> 30);
-        bool neg = false;
-        if (lane < 4 && (at(tn, lane) >> 2) != prev) {
-            const Pt q[4] = {vpt(vx, tv.x), vpt(vx, tv.y), vpt(vx, tv.z), vpt(vx, tv.w)};
-            neg = orient_replaced(q, lane, p, st) < 0;
-        }
-        const unsigned m = __ballot_sync(kFull, neg) & 0xFu;
-        *nsteps = step + 1;
-        if (m == 0) return t;
-        const unsigned rot = ((m >> s0) | (m << (4 - s0))) & 0xFu;
-        const int i = (s0 + __ffs(int(rot)) - 1) & 3;
-        const int next = at(tn, i) >> 2;
-        const int4 nv = T.tv[next];
-        if (inf_pos(nv) >= 0) return next;
-        prev = t;
-        t = next;
-        tv = nv;
-    }
-    report(st, ST_WALK_LIMIT);
-    return -1;
-}
-
 /// Advances worker w to the next point of its chunk (walked cyclically),
 /// skipping its set's first-tet vertices; -1 when the chunk is done.
 __device__ int next_point(const Workers& W, int w) {
@@ -250,57 +211,153 @@ __device__ int next_point(const Workers& W, int w) {
     return v;
 }
 
-/// One warp per worker: locate the worker's point, then grow its conflict
-/// region breadth-first, eight region tets (32 facets) per step, claiming
+// ---- the insertion kernels ---------------------------------------------------
+//
+// A worker is served by a group of G lanes (G = 32, 16, 8 or 4), so one warp
+// serves 32 / G workers side by side.  Few workers: G = 32 shortens each
+// worker's chain of dependent memory accesses (8 region tets per step).  Many
+// workers (more than the GPU keeps resident as warps): a small G packs them into
+// fewer warps, so the whole round fits the resident warps and its time is one
+// chain instead of several waves of chains.  Control flow stays uniform over
+// the warp - every loop runs until all of its groups are done - so the groups'
+// memory accesses are issued together and warp votes cover all 32 lanes; a
+// group reads its own bits of each vote.
+
+template <int G>
+struct Lanes {
+    int lane, sub, gbase;
+    unsigned gm;   // the group's bits in a warp-wide vote
+    __device__ Lanes() {
+        lane = threadIdx.x & 31;
+        sub = lane & (G - 1);
+        gbase = lane - sub;
+        gm = G == 32 ? kFull : (((1u << G) - 1u) << gbase);
+    }
+    /// The group's bits of a warp-wide vote, lane 0 of the group at bit 0.
+    __device__ unsigned own(unsigned vote) const { return G == 32 ? vote : (vote & gm) >> gbase; }
+};
+
+/// Visibility walk from each live group's start tet to a tet in conflict with
+/// its point p: the finite tet containing p, or the infinite tet beyond the hull
+/// facet the walk crosses.  Lanes 0-3 of a group test the four facets of a step;
+/// the first negative one in a pseudo-random cyclic order is crossed (never the
+/// facet just crossed).  Returns the tet (same in every lane of the group), or
+/// -1 for a group that is not live or hit the walk limit.
+template <int G>
+__device__ int walk_g(bool live, int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
+                      uint32_t* st, const Lanes<G>& L, int* nsteps) {
+    int4 tv = make_int4(0, 0, 0, 0);
+    if (live) {
+        tv = T.tv[t];
+        const int ip = inf_pos(tv);
+        if (ip >= 0) {
+            t = at(T.tn[t], ip) >> 2;
+            tv = T.tv[t];
+        }
+    }
+    int prev = -1, found = -1;
+    uint32_t h = uint32_t(pid) * 2654435761u + 12345u;
+    bool walking = live;
+    for (int step = 0; __any_sync(kFull, walking); ++step) {
+        int4 tn = make_int4(0, 0, 0, 0);
+        bool neg = false;
+        if (walking) {
+            tn = T.tn[t];
+            h = h * 1664525u + 1013904223u;
+            if (L.sub < 4 && (at(tn, L.sub) >> 2) != prev) {
+                const Pt q[4] = {vpt(vx, tv.x), vpt(vx, tv.y), vpt(vx, tv.z), vpt(vx, tv.w)};
+                neg = orient_replaced(q, L.sub, p, st) < 0;
+            }
+        }
+        const unsigned m = L.own(__ballot_sync(kFull, neg)) & 0xFu;
+        if (walking) {
+            *nsteps = step + 1;
+            if (m == 0) {
+                found = t;
+                walking = false;
+            } else {
+                const int s0 = int(h >> 30);
+                const unsigned rot = ((m >> s0) | (m << (4 - s0))) & 0xFu;
+                const int i = (s0 + __ffs(int(rot)) - 1) & 3;
+                const int next = at(tn, i) >> 2;
+                const int4 nv = T.tv[next];
+                if (inf_pos(nv) >= 0) {
+                    found = next;
+                    walking = false;
+                } else {
+                    prev = t;
+                    t = next;
+                    tv = nv;
+                    if (step + 1 >= kWalkLimit) {
+                        report(st, ST_WALK_LIMIT);
+                        walking = false;
+                    }
+                }
+            }
+        }
+    }
+    return found;
+}
+
+/// One group of G lanes per worker: locate the worker's point, then grow its
+/// conflict region breadth-first, G/4 region tets (G facets) per step, claiming
 /// every region tet (key) and every tet across the region boundary (key|1).
+template <int G>
 __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R, const double* __restrict__ vx,
                                                 int first) {
-    const int lane = threadIdx.x & 31;
-    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (slot >= W.n) return;
-    const int w = W.list ? W.list[slot] : slot;
-    const int v = W.cur[w];
-    // Normal rounds leave parked workers alone; big rounds serve only those.
-    if (v < 0 || (W.parked[w] != 0) != (W.list != nullptr)) {
-        if (lane == 0) W.state[w] = v < 0 ? WS_DONE : WS_PARKED;
-        return;
+    const Lanes<G> L;
+    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) / G);
+    bool live = slot < W.n;
+    int w = 0, v = -1;
+    if (live) {
+        w = W.list ? W.list[slot] : slot;
+        v = W.cur[w];
+        // Normal rounds leave parked workers alone; big rounds serve only those.
+        if (v < 0 || (W.parked[w] != 0) != (W.list != nullptr)) {
+            if (L.sub == 0) W.state[w] = v < 0 ? WS_DONE : WS_PARKED;
+            live = false;
+        }
     }
-    const Pt p = vpt(vx, v);
-    const int sv = W.last[w] >= 0 ? W.last[w] : W.guide[w];
+    if (!__any_sync(kFull, live)) return;
+    const Pt p = live ? vpt(vx, v) : Pt{0.0, 0.0, 0.0};
+    int start = 0;
+    if (live) start = T.vert_tet[W.last[w] >= 0 ? W.last[w] : W.guide[w]];
     int wsteps = 0;
-    const int seed = walk_w(T.vert_tet[sv], p, v, T, vx, R.status, lane, &wsteps);
-    if (R.steps && lane == 0) atomicAdd(R.steps, (unsigned long long)wsteps);
-    if (seed < 0) {
-        if (lane == 0) W.state[w] = WS_FAIL;
-        return;
+    const int seed = walk_g<G>(live, start, p, v, T, vx, R.status, L, &wsteps);
+    if (R.steps && live && L.sub == 0) atomicAdd(R.steps, (unsigned long long)wsteps);
+    if (live && seed < 0) {
+        if (L.sub == 0) W.state[w] = WS_FAIL;
+        live = false;
     }
-    const unsigned long long key = claim_key(R, v);
+    const unsigned long long key = live ? claim_key(R, v) : 0ull;
     const unsigned long long mine = key >> 1;
-    int* cav = W.cav + int64_t(slot) * W.cav_cap;
-    int* fac = W.fac + int64_t(slot) * W.fac_cap;
+    int* cav = W.cav + int64_t(live ? slot : 0) * W.cav_cap;
+    int* fac = W.fac + int64_t(live ? slot : 0) * W.fac_cap;
     int lost = 0;
-    if (lane == 0) {
+    if (live && L.sub == 0) {
         const unsigned long long old = atomicMin(T.claim + seed, key);
         lost = (old >> 1) < mine;
         cav[0] = seed;
     }
-    if (__shfl_sync(kFull, lost, 0)) {
-        if (lane == 0) W.state[w] = WS_LOST;
-        return;
+    lost = __shfl_sync(kFull, lost, L.gbase);
+    if (live && lost) {
+        if (L.sub == 0) W.state[w] = WS_LOST;
+        live = false;
     }
     __syncwarp();
-    const unsigned lt = (1u << lane) - 1u;
+    const unsigned lt = (1u << L.lane) - 1u;
     int ncav = 1, nfac = 0, head = 0;
-    while (head < ncav) {
-        if (R.steps && lane == 0) atomicAdd(R.steps + 1, 1ull);
-        const int nproc = min(ncav - head, 8);
-        const bool valid = (lane >> 2) < nproc;
-        const int i = lane & 3;
+    bool growing = live;
+    while (__any_sync(kFull, growing)) {
+        if (R.steps && growing && L.sub == 0) atomicAdd(R.steps + 1, 1ull);
+        const int nproc = growing ? min(ncav - head, G / 4) : 0;
+        const bool valid = (L.sub >> 2) < nproc;
+        const int i = L.sub & 3;
         int c = 0, nb = 0;
         int kind = 0;   // 0: nothing, 1: boundary facet, 2: new region tet, 3: re-check
         bool abort = false;
         if (valid) {
-            c = cav[head + (lane >> 2)];
+            c = cav[head + (L.sub >> 2)];
             nb = at(T.tn[c], i) >> 2;
             const unsigned long long old = atomicMin(T.claim + nb, key | 1ull);
             if (old == key) {
@@ -317,26 +374,28 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
                 kind = 1;
             }
         }
-        if (__any_sync(kFull, abort)) {
-            if (lane == 0) W.state[w] = WS_LOST;
-            return;
+        const unsigned ab0 = L.own(__ballot_sync(kFull, abort));
+        if (growing && ab0) {
+            if (L.sub == 0) W.state[w] = WS_LOST;
+            growing = false;
         }
         __syncwarp();
-        if (kind == 3) {
+        if (growing && kind == 3) {
             // Another lane of this step may have just turned it into a region tet.
             const unsigned long long now = __ldcg(T.claim + nb);
             if (now == key) kind = 0;
             else if ((now >> 1) < mine) abort = true;
             else kind = 1;
         }
-        if (__any_sync(kFull, abort)) {
-            if (lane == 0) W.state[w] = WS_LOST;
-            return;
+        const unsigned ab = L.own(__ballot_sync(kFull, growing && abort));
+        if (growing && ab) {
+            if (L.sub == 0) W.state[w] = WS_LOST;
+            growing = false;
         }
-        const unsigned mc = __ballot_sync(kFull, kind == 2);
-        const unsigned mf = __ballot_sync(kFull, kind == 1);
-        if (ncav + __popc(mc) > W.cav_cap || nfac + __popc(mf) > W.fac_cap) {
-            if (lane == 0) {
+        const unsigned mc = __ballot_sync(kFull, growing && kind == 2) & L.gm;
+        const unsigned mf = __ballot_sync(kFull, growing && kind == 1) & L.gm;
+        if (growing && (ncav + __popc(mc) > W.cav_cap || nfac + __popc(mf) > W.fac_cap)) {
+            if (L.sub == 0) {
                 // Too big for this scratch: park the worker until a big round
                 // (or, in a big round, report that even that was not enough).
                 W.state[w] = WS_PARKED;
@@ -344,81 +403,130 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
                 else W.parked[w] = 1;
                 atomicAdd(R.counters + 3, 1);   // its claims may have blocked others
             }
-            return;
+            growing = false;
         }
-        if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
-        if (kind == 1) fac[nfac + __popc(mf & lt)] = c * 4 + i;
-        ncav += __popc(mc);
-        nfac += __popc(mf);
-        head += nproc;
+        if (growing) {
+            if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
+            if (kind == 1) fac[nfac + __popc(mf & lt)] = c * 4 + i;
+            ncav += __popc(mc);
+            nfac += __popc(mf);
+            head += nproc;
+            if (head >= ncav) {
+                if (L.sub == 0) {
+                    W.ncav[w] = ncav;
+                    W.nfac[w] = nfac;
+                    W.state[w] = WS_CAND;
+                }
+                growing = false;
+            }
+        }
         __syncwarp();
     }
-    if (lane == 0) {
-        W.ncav[w] = ncav;
-        W.nfac[w] = nfac;
-        W.state[w] = WS_CAND;
-    }
 }
 
-/// One warp per candidate: it wins if it still holds every claim it made.
+/// One group per candidate: it wins if it still holds every claim it made.
+template <int G>
 __global__ void __launch_bounds__(128, 8) k_check(Tables T, Workers W, Round R, int first) {
-    const int lane = threadIdx.x & 31;
-    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (slot >= W.n) return;
-    const int w = W.list ? W.list[slot] : slot;
-    if (W.state[w] != WS_CAND) return;
-    const int v = W.cur[w];
-    const unsigned long long key = claim_key(R, v);
-    const int* cav = W.cav + int64_t(slot) * W.cav_cap;
-    const int* fac = W.fac + int64_t(slot) * W.fac_cap;
-    const int ncav = W.ncav[w], nfac = W.nfac[w];
-    bool ok = true;
-    for (int k = lane; k < ncav; k += 32) ok = ok && T.claim[cav[k]] == key;
-    for (int k = lane; k < nfac; k += 32) {
-        const int f = fac[k];
-        ok = ok && T.claim[at(T.tn[f >> 2], f & 3) >> 2] == (key | 1ull);
+    const Lanes<G> L;
+    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) / G);
+    bool live = slot < W.n;
+    int w = 0;
+    if (live) {
+        w = W.list ? W.list[slot] : slot;
+        live = W.state[w] == WS_CAND;
     }
-    const bool win = __all_sync(kFull, ok);
-    if (lane == 0) W.state[w] = win ? WS_WIN : WS_LOST;
+    if (!__any_sync(kFull, live)) return;
+    bool ok = true;
+    if (live) {
+        const int v = W.cur[w];
+        const unsigned long long key = claim_key(R, v);
+        const int* cav = W.cav + int64_t(slot) * W.cav_cap;
+        const int* fac = W.fac + int64_t(slot) * W.fac_cap;
+        const int ncav = W.ncav[w], nfac = W.nfac[w];
+        for (int k = L.sub; k < ncav; k += G) ok = ok && T.claim[cav[k]] == key;
+        for (int k = L.sub; k < nfac; k += G) {
+            const int f = fac[k];
+            ok = ok && T.claim[at(T.tn[f >> 2], f & 3) >> 2] == (key | 1ull);
+        }
+    }
+    const bool win = L.own(__ballot_sync(kFull, !ok)) == 0;
+    if (live && L.sub == 0) W.state[w] = win ? WS_WIN : WS_LOST;
 }
 
-/// One warp per winner: re-star its region, one boundary facet per lane.
+/// Neighbour of new tet facet j (the new tet replaces facet i of region tet c):
+/// facet j is {v} + edge (va, vb), and its neighbour is the new tet on the other
+/// boundary facet through that edge, reached by turning around the edge inside
+/// the region (reference src/tds.h:160-221).  Returns the encoded neighbour
+/// (tet * 4 + facet), or -1 if the region is inconsistent.
+__device__ int restar_neighbour(const Tables& T, int c, const int4& cv, int i, int j,
+                                unsigned long long key) {
+    int a = -1, b = -1;
+    for (int m = 0; m < 4; ++m)
+        if (m != i && m != j) {
+            if (a < 0) a = m;
+            else b = m;
+        }
+    const int va = at(cv, a), vb = at(cv, b);
+    int cur = c, f = j, steps = 0;
+    for (;;) {
+        const int enc = at(T.tn[cur], f);
+        const int nb = enc >> 2;
+        if (T.claim[nb] != key) {   // (cur, f) is a boundary facet
+            const int4 tc = T.tv[cur];
+            const int wpos = 6 - f - pos_of(tc, va) - pos_of(tc, vb);
+            if (wpos < 0 || wpos > 3 || wpos == f) return -1;
+            return T.fnew[cur * 4 + f] * 4 + wpos;
+        }
+        const int4 tb = T.tv[nb];
+        const int g = enc & 3;
+        f = 6 - g - pos_of(tb, va) - pos_of(tb, vb);
+        cur = nb;
+        if (f < 0 || f > 3 || f == g || ++steps > kRotateLimit) return -1;
+    }
+}
+
+/// One group per winner: re-star its region, one boundary facet per lane.
+template <int G>
 __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R, int first) {
     __shared__ int sh_count[3];
-    const int lane = threadIdx.x & 31;
-    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const Lanes<G> L;
+    const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) / G);
     if (threadIdx.x < 3) sh_count[threadIdx.x] = 0;
     __syncthreads();
     const bool exists = slot < W.n;
     const int w = exists ? (W.list ? W.list[slot] : slot) : 0;
     const int state = exists ? W.state[w] : WS_DONE;
     const int v = exists ? W.cur[w] : -1;
+    const bool winner = state == WS_WIN;
     bool advanced = false;
-    if (state == WS_WIN) {
-        const unsigned long long key = claim_key(R, v);
-        const int* cav = W.cav + int64_t(slot) * W.cav_cap;
-        const int* fac = W.fac + int64_t(slot) * W.fac_cap;
-        int4* sv = W.st_v + int64_t(slot) * W.fac_cap;
-        int4* sn = W.st_n + int64_t(slot) * W.fac_cap;
-        const int C = W.ncav[w], F = W.nfac[w];
+    if (__any_sync(kFull, winner)) {
+        const unsigned long long key = winner ? claim_key(R, v) : 0ull;
+        const int64_t sl = winner ? slot : 0;
+        const int* cav = W.cav + sl * W.cav_cap;
+        const int* fac = W.fac + sl * W.fac_cap;
+        int4* sv = W.st_v + sl * W.fac_cap;
+        int4* sn = W.st_n + sl * W.fac_cap;
+        const int C = winner ? W.ncav[w] : 0, F = winner ? W.nfac[w] : 0;
         const int extra = F > C ? F - C : 0;
-        int base = 0, ok = 1;
-        if (lane == 0 && extra > 0) {
+        int base = 0, ok = winner ? 1 : 0;
+        if (winner && L.sub == 0 && extra > 0) {
             base = atomicAdd(T.tet_count, extra);
             if (base + extra > T.cap) {
                 report(R.status, ST_TET_CAPACITY);
                 ok = 0;
             }
         }
-        base = __shfl_sync(kFull, base, 0);
-        ok = __shfl_sync(kFull, ok, 0);
-        if (ok) {
-            // 1a: the new tet of each boundary facet.
-            for (int k = lane; k < F; k += 32) T.fnew[fac[k]] = k < C ? cav[k] : base + (k - C);
-            __syncwarp();
-            // 1b: vertices and neighbours, from the region as it was.
-            bool bad = false;
-            for (int k = lane; k < F && !bad; k += 32) {
+        base = __shfl_sync(kFull, base, L.gbase);
+        ok = __shfl_sync(kFull, ok, L.gbase);
+        // 1a: the new tet of each boundary facet.
+        if (ok)
+            for (int k = L.sub; k < F; k += G) T.fnew[fac[k]] = k < C ? cav[k] : base + (k - C);
+        __syncwarp();
+        // 1b: vertices and neighbours, from the region as it was.
+        bool bad = false;
+        for (int k0 = 0; __any_sync(kFull, ok && k0 < F); k0 += G) {
+            const int k = k0 + L.sub;
+            if (ok && k < F) {
                 const int c = fac[k] >> 2, i = fac[k] & 3;
                 const int4 cv = T.tv[c];
                 const int4 cn = T.tn[c];
@@ -426,49 +534,22 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
                 set_at(nv, i, v);
                 for (int j = 0; j < 4 && !bad; ++j) {
                     if (j == i) continue;
-                    // Facet j of the new tet is {v} + edge (va, vb); its neighbour is
-                    // the new tet on the other boundary facet through that edge,
-                    // reached by turning around the edge inside the region.
-                    int a = -1, b = -1;
-                    for (int m = 0; m < 4; ++m)
-                        if (m != i && m != j) {
-                            if (a < 0) a = m;
-                            else b = m;
-                        }
-                    const int va = at(cv, a), vb = at(cv, b);
-                    int cur = c, f = j, steps = 0;
-                    for (;;) {
-                        const int enc = at(T.tn[cur], f);
-                        const int nb = enc >> 2;
-                        if (T.claim[nb] != key) {   // (cur, f) is a boundary facet
-                            const int4 tc = T.tv[cur];
-                            const int wpos = 6 - f - pos_of(tc, va) - pos_of(tc, vb);
-                            if (wpos < 0 || wpos > 3 || wpos == f) bad = true;
-                            else set_at(nn, j, T.fnew[cur * 4 + f] * 4 + wpos);
-                            break;
-                        }
-                        const int4 tb = T.tv[nb];
-                        const int g = enc & 3;
-                        f = 6 - g - pos_of(tb, va) - pos_of(tb, vb);
-                        cur = nb;
-                        if (f < 0 || f > 3 || f == g || ++steps > kRotateLimit) {
-                            bad = true;
-                            break;
-                        }
-                    }
+                    const int e = restar_neighbour(T, c, cv, i, j, key);
+                    if (e < 0) bad = true;
+                    else set_at(nn, j, e);
                 }
                 sv[k] = nv;
                 sn[k] = nn;
             }
-            if (__any_sync(kFull, bad)) {
-                if (lane == 0) report(R.status, ST_INTERNAL);
-                ok = 0;
-            }
-            __syncwarp();
         }
+        if (L.own(__ballot_sync(kFull, bad))) {
+            if (L.sub == 0) report(R.status, ST_INTERNAL);
+            ok = 0;
+        }
+        __syncwarp();
         if (ok) {
             // 2: write the new tets and re-point the outside neighbours.
-            for (int k = lane; k < F; k += 32) {
+            for (int k = L.sub; k < F; k += G) {
                 const int id = k < C ? cav[k] : base + (k - C);
                 const int4 nv = sv[k], nn = sn[k];
                 const int i = fac[k] & 3;
@@ -482,15 +563,15 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
                 if (nv.z != kInf) T.vert_tet[nv.z] = id;
                 if (nv.w != kInf) T.vert_tet[nv.w] = id;
             }
-            for (int k = F + lane; k < C; k += 32) T.alive[cav[k]] = 0;
+            for (int k = F + L.sub; k < C; k += G) T.alive[cav[k]] = 0;
             advanced = true;
-            if (lane == 0) {
+            if (L.sub == 0) {
                 atomicAdd(R.sums, (unsigned long long)C);
                 atomicAdd(R.sums + 1, (unsigned long long)F);
             }
         }
     }
-    if (lane == 0 && exists) {
+    if (L.sub == 0 && exists) {
         int cur = v;
         if (advanced) {
             W.last[w] = v;
@@ -509,6 +590,425 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
         if (sh_count[2]) atomicAdd(R.counters + 2, sh_count[2]);
     }
 }
+
+// ---- asynchronous insertion --------------------------------------------------
+//
+// The rounds above insert in lockstep: every round waits for its slowest
+// worker.  k_insert_async lets every warp run at its own pace instead.  A
+// persistent grid of warps takes the level's chunks from a queue and inserts
+// their points one after another.  An insertion try-locks every tet it reads
+// to decide its conflict region - the region tets and the tets across the
+// region boundary - and holds the locks until its new tets are written, so
+// insertions whose locks succeed touch disjoint tets and commute: the result
+// is that of some sequential order, hence (the tet set does not depend on the
+// insertion order) the canonical set.  A lock held by another warp makes the
+// insertion give back its locks and try again after a back-off; after a few
+// failures, and for a conflict region too large for the warp's scratch, the
+// point is left for the rounds, which finish it.  No warp ever waits while it
+// holds a lock, and every loop is bounded.
+//
+// Lock word of a tet: 0 free, else (owner << 1) | ring, owner = warp slot + 1;
+// ring = 1 for a tet across the region boundary, 0 for a region tet.  Locks are
+// taken with acquire and released with release ordering, and every read of
+// tet data that other warps write goes to L2 (__ldcg), not the SM's L1.
+
+constexpr int kAsyncRetries = 6;
+constexpr int kAsyncWalkLimit = 1 << 14;
+
+struct AsyncCtx {
+    int* lock;                      // per tet lock word
+    int* next;                      // chunk queue head
+    int* leftover;                  // points left for the rounds
+    int* n_leftover;
+    int64_t stride;                 // chunk q of the queue is chunk (q * stride) % W.n
+    unsigned long long* stats;      // [0] lock conflicts, [1] walk restarts
+};
+
+using LockRef = cuda::atomic_ref<int, cuda::thread_scope_device>;
+
+__device__ __forceinline__ bool try_lock(int* lock, int t, int value, int* seen) {
+    int expected = 0;
+    const bool ok = LockRef(lock[t]).compare_exchange_strong(expected, value, cuda::memory_order_acquire,
+                                                             cuda::memory_order_relaxed);
+    *seen = ok ? 0 : expected;
+    return ok;
+}
+
+/// Releases tet t if `value` still holds it (a ring tet may be listed twice).
+__device__ __forceinline__ void unlock_if(int* lock, int t, int value) {
+    int expected = value;
+    LockRef(lock[t]).compare_exchange_strong(expected, 0, cuda::memory_order_release, cuda::memory_order_relaxed);
+}
+
+__device__ __forceinline__ int4 ld4(const int4* p) { return __ldcg(p); }
+
+/// Visibility walk on a mesh other warps are changing: reads go to L2 and may
+/// be stale, so the tet it returns is only a candidate, checked under its lock.
+/// Returns -1 after kAsyncWalkLimit steps.
+__device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
+                          uint32_t* st, int lane) {
+    int4 tv = ld4(T.tv + t);
+    {
+        const int ip = inf_pos(tv);
+        if (ip >= 0) {
+            t = at(ld4(T.tn + t), ip) >> 2;
+            tv = ld4(T.tv + t);
+        }
+    }
+    int prev = -1;
+    uint32_t h = uint32_t(pid) * 2654435761u + 12345u;
+    for (int step = 0; step < kAsyncWalkLimit; ++step) {
+        const int4 tn = ld4(T.tn + t);
+        h = h * 1664525u + 1013904223u;
+        const int s0 = int(h >> 30);
+        bool neg = false;
+        if (lane < 4 && (at(tn, lane) >> 2) != prev && tv.x != kInf && tv.y != kInf && tv.z != kInf &&
+            tv.w != kInf) {
+            const Pt q[4] = {vpt(vx, tv.x), vpt(vx, tv.y), vpt(vx, tv.z), vpt(vx, tv.w)};
+            neg = orient_replaced(q, lane, p, st) < 0;
+        }
+        const unsigned m = __ballot_sync(kFull, neg) & 0xFu;
+        if (m == 0) return t;
+        const unsigned rot = ((m >> s0) | (m << (4 - s0))) & 0xFu;
+        const int i = (s0 + __ffs(int(rot)) - 1) & 3;
+        const int next = at(tn, i) >> 2;
+        const int4 nv = ld4(T.tv + next);
+        if (inf_pos(nv) >= 0) return next;
+        prev = t;
+        t = next;
+        tv = nv;
+    }
+    return -1;
+}
+
+/// Neighbour across facet j of the new tet built on facet i of locked region
+/// tet c (see restar_neighbour); region membership is read from the locks.
+__device__ int restar_neighbour_locked(const Tables& T, const int* lock, int region, int c, const int4& cv,
+                                       int i, int j) {
+    int a = -1, b = -1;
+    for (int m = 0; m < 4; ++m)
+        if (m != i && m != j) {
+            if (a < 0) a = m;
+            else b = m;
+        }
+    const int va = at(cv, a), vb = at(cv, b);
+    int cur = c, f = j, steps = 0;
+    for (;;) {
+        const int enc = at(ld4(T.tn + cur), f);
+        const int nb = enc >> 2;
+        if (__ldcg(lock + nb) != region) {   // (cur, f) is a boundary facet
+            const int4 tc = ld4(T.tv + cur);
+            const int wpos = 6 - f - pos_of(tc, va) - pos_of(tc, vb);
+            if (wpos < 0 || wpos > 3 || wpos == f) return -1;
+            return __ldcg(T.fnew + cur * 4 + f) * 4 + wpos;
+        }
+        const int4 tb = ld4(T.tv + nb);
+        const int g = enc & 3;
+        f = 6 - g - pos_of(tb, va) - pos_of(tb, vb);
+        cur = nb;
+        if (f < 0 || f > 3 || f == g || ++steps > kRotateLimit) return -1;
+    }
+}
+
+enum : int { AI_DONE = 0, AI_RETRY = 1, AI_LEAVE = 2 };
+
+/// One insertion of point v by the whole warp, starting the walk at tet t0.
+/// AI_DONE: inserted; AI_RETRY: a lock was taken by another warp (nothing
+/// changed, every lock given back); AI_LEAVE: leave it for the rounds.
+__device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, const AsyncCtx& A,
+                            const double* __restrict__ vx, uint32_t* st, int slot, int lane,
+                            unsigned long long* nC, unsigned long long* nF) {
+    const int owner = slot + 1;
+    const int region = owner << 1, ring = region | 1;
+    const Pt p = vpt(vx, v);
+    const int seed = walk_async(t0, p, v, T, vx, st, lane);
+    if (seed < 0) {
+        if (lane == 0) atomicAdd(A.stats + 1, 1ull);
+        return AI_RETRY;
+    }
+    int* cav = W.cav + int64_t(slot) * W.cav_cap;
+    int* fac = W.fac + int64_t(slot) * W.fac_cap;
+    // Seed: lock it, then check under the lock that it is alive and in conflict.
+    int res = 0;   // 0 ok, 1 lock held by another, 2 not a valid seed
+    if (lane == 0) {
+        int seen = 0;
+        if (!try_lock(A.lock, seed, region, &seen)) {
+            res = 1;
+        } else if (!__ldcg(T.alive + seed) || !in_conflict(ld4(T.tv + seed), p, v, vx, st)) {
+            unlock_if(A.lock, seed, region);
+            res = 2;
+        } else {
+            cav[0] = seed;
+        }
+    }
+    res = __shfl_sync(kFull, res, 0);
+    if (res != 0) {
+        if (res == 1 && lane == 0) atomicAdd(A.stats, 1ull);
+        return AI_RETRY;
+    }
+    __syncwarp();
+    const unsigned lt = (1u << lane) - 1u;
+    int ncav = 1, nfac = 0, head = 0;
+    int outcome = AI_DONE;
+    while (head < ncav) {
+        const int nproc = min(ncav - head, 8);
+        const bool valid = (lane >> 2) < nproc;
+        const int i = lane & 3;
+        int c = 0, nb = 0, kind = 0, got = -1;   // got: a tet this lane locked in this step
+        bool abort = false;
+        if (valid) {
+            c = cav[head + (lane >> 2)];
+            nb = at(ld4(T.tn + c), i) >> 2;
+            int seen = 0;
+            if (try_lock(A.lock, nb, ring, &seen)) {
+                got = nb;
+                if (in_conflict(ld4(T.tv + nb), p, v, vx, st)) {
+                    LockRef(A.lock[nb]).store(region, cuda::memory_order_relaxed);
+                    kind = 2;
+                } else {
+                    kind = 1;
+                }
+            } else if (seen == region) {
+                kind = 0;                                 // already in the region
+            } else if (seen == ring) {
+                kind = 3;                                 // locked by us this step: decided below
+            } else {
+                abort = true;                             // another warp holds it
+            }
+        }
+        __syncwarp();
+        if (kind == 3) kind = __ldcg(A.lock + nb) == region ? 0 : 1;
+        const bool ab = __any_sync(kFull, abort);
+        const unsigned mc = __ballot_sync(kFull, kind == 2);
+        const unsigned mf = __ballot_sync(kFull, kind == 1);
+        const bool full = ncav + __popc(mc) > W.cav_cap || nfac + __popc(mf) > W.fac_cap;
+        if (ab || full) {
+            // Give everything back: this step's new locks, the region, the ring.
+            if (got >= 0) unlock_if(A.lock, got, kind == 2 ? region : ring);
+            __syncwarp();
+            for (int k = lane; k < nfac; k += 32) {
+                const int f = fac[k];
+                unlock_if(A.lock, at(ld4(T.tn + (f >> 2)), f & 3) >> 2, ring);
+            }
+            __syncwarp();
+            for (int k = lane; k < ncav; k += 32) unlock_if(A.lock, cav[k], region);
+            if (lane == 0 && ab) atomicAdd(A.stats, 1ull);
+            outcome = ab ? AI_RETRY : AI_LEAVE;
+            break;
+        }
+        if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
+        if (kind == 1) fac[nfac + __popc(mf & lt)] = c * 4 + i;
+        ncav += __popc(mc);
+        nfac += __popc(mf);
+        head += nproc;
+        __syncwarp();
+    }
+    if (outcome != AI_DONE) return outcome;
+
+    // Re-star (as k_restar), reading the locked region through L2.
+    const int C = ncav, F = nfac;
+    const int extra = F > C ? F - C : 0;
+    int base = 0, ok = 1;
+    if (lane == 0 && extra > 0) {
+        base = atomicAdd(T.tet_count, extra);
+        if (base + extra > T.cap) {
+            report(st, ST_TET_CAPACITY);
+            ok = 0;
+        }
+    }
+    base = __shfl_sync(kFull, base, 0);
+    ok = __shfl_sync(kFull, ok, 0);
+    int4* sv = W.st_v + int64_t(slot) * W.fac_cap;
+    int4* sn = W.st_n + int64_t(slot) * W.fac_cap;
+    // Fresh slots are locked too, so that whoever locks one later reads it only
+    // after this warp's release.  A stale walk of another warp may hold one for
+    // a moment (it finds it not alive and lets go): wait for that, bounded.
+    bool locked_fresh = true;
+    if (ok) {
+        for (int k = C + lane; k < F; k += 32) {
+            int seen = 0;
+            bool got = false;
+            for (int it = 0; it < (1 << 16) && !got; ++it) {
+                got = try_lock(A.lock, base + (k - C), region, &seen);
+                if (!got) __nanosleep(128);
+            }
+            locked_fresh = locked_fresh && got;
+        }
+        if (!__all_sync(kFull, locked_fresh)) {
+            for (int k = C + lane; k < F; k += 32) unlock_if(A.lock, base + (k - C), region);
+            if (lane == 0) report(st, ST_INTERNAL);
+            ok = 0;
+        }
+    }
+    if (ok) {
+        for (int k = lane; k < F; k += 32) T.fnew[fac[k]] = k < C ? cav[k] : base + (k - C);
+        __syncwarp();
+        bool bad = false;
+        for (int k = lane; k < F && !bad; k += 32) {
+            const int c = fac[k] >> 2, i = fac[k] & 3;
+            const int4 cv = ld4(T.tv + c);
+            int4 nv = cv, nn = ld4(T.tn + c);
+            set_at(nv, i, v);
+            for (int j = 0; j < 4 && !bad; ++j) {
+                if (j == i) continue;
+                const int e = restar_neighbour_locked(T, A.lock, region, c, cv, i, j);
+                if (e < 0) bad = true;
+                else set_at(nn, j, e);
+            }
+            sv[k] = nv;
+            sn[k] = nn;
+        }
+        if (__any_sync(kFull, bad)) {
+            if (lane == 0) report(st, ST_INTERNAL);
+            ok = 0;
+        }
+        __syncwarp();
+    }
+    if (ok) {
+        for (int k = lane; k < F; k += 32) {
+            const int id = k < C ? cav[k] : base + (k - C);
+            const int4 nv = sv[k], nn = sn[k];
+            const int i = fac[k] & 3;
+            T.tv[id] = nv;
+            T.tn[id] = nn;
+            T.alive[id] = 1;
+            const int enc = at(nn, i);
+            reinterpret_cast<int*>(T.tn)[(enc >> 2) * 4 + (enc & 3)] = id * 4 + i;
+            if (nv.x != kInf) T.vert_tet[nv.x] = id;
+            if (nv.y != kInf) T.vert_tet[nv.y] = id;
+            if (nv.z != kInf) T.vert_tet[nv.z] = id;
+            if (nv.w != kInf) T.vert_tet[nv.w] = id;
+        }
+        for (int k = F + lane; k < C; k += 32) T.alive[cav[k]] = 0;
+    }
+    // Publish, then give the locks back (ring tets first: their neighbour
+    // entries now point at the new tets).
+    __threadfence();
+    __syncwarp();
+    for (int k = lane; k < F; k += 32) {
+        const int f = fac[k];
+        const int c = f >> 2, i = f & 3;
+        // The outside tet across facet (c, i): read from the staged neighbours,
+        // since slot c may now hold a new tet.
+        const int outside = ok ? (at(sn[k], i) >> 2) : (at(ld4(T.tn + c), i) >> 2);
+        unlock_if(A.lock, outside, ring);
+    }
+    __syncwarp();
+    for (int k = lane; k < C; k += 32) unlock_if(A.lock, cav[k], region);
+    if (ok)
+        for (int k = C + lane; k < F; k += 32) unlock_if(A.lock, base + (k - C), region);
+    if (lane == 0) {
+        *nC += (unsigned long long)C;
+        *nF += (unsigned long long)F;
+    }
+    return ok ? AI_DONE : AI_LEAVE;
+}
+
+/// Persistent warps over a level's chunks (set up by k_setup_level).
+__global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, AsyncCtx A, Round R,
+                                                      const double* __restrict__ vx, int nslots) {
+    const int lane = threadIdx.x & 31;
+    const int slot = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (slot >= nslots) return;   // the grid is rounded up to whole blocks; scratch has nslots slots
+    unsigned long long won = 0, tries = 0, nC = 0, nF = 0;
+    for (;;) {
+        int q = 0;
+        if (lane == 0) q = atomicAdd(A.next, 1);
+        q = __shfl_sync(kFull, q, 0);
+        if (q >= W.n) break;
+        const int w = int((int64_t(q) * A.stride) % W.n);
+        const int b = W.beg[w], len = W.end[w] - b;
+        const int4 sk = W.skips[W.wset[w]];
+        int pos = W.pos[w], left = W.left[w];
+        int v = W.cur[w];
+        int last = -1;
+        const int guide = W.guide[w];
+        while (v >= 0) {
+            int outcome = AI_RETRY;
+            for (int attempt = 0; attempt < kAsyncRetries && outcome == AI_RETRY; ++attempt) {
+                if (attempt > 0) __nanosleep(200u << min(attempt, 6));
+                const int t0 = __ldcg(T.vert_tet + (last >= 0 ? last : guide));
+                outcome = insert_async(v, t0, T, W, A, vx, R.status, slot, lane, &nC, &nF);
+                ++tries;
+                if (__ldcg(R.status) != 0) outcome = AI_LEAVE;
+            }
+            if (outcome == AI_DONE) {
+                ++won;
+                last = v;
+            } else if (lane == 0) {
+                A.leftover[atomicAdd(A.n_leftover, 1)] = v;
+            }
+            if (__ldcg(R.status) != 0) break;
+            // next point of the chunk (as next_point)
+            v = -1;
+            while (left > 0) {
+                const int c = b + pos;
+                pos = pos + 1 == len ? 0 : pos + 1;
+                --left;
+                if (c != sk.x && c != sk.y && c != sk.z && c != sk.w) {
+                    v = c;
+                    break;
+                }
+            }
+        }
+        if (__ldcg(R.status) != 0) break;
+    }
+    if (lane == 0) {
+        atomicAdd(R.totals, won);
+        atomicAdd(R.totals + 1, tries);
+        atomicAdd(R.sums, nC);
+        atomicAdd(R.sums + 1, nF);
+    }
+}
+
+/// Workers for the points the asynchronous pass left: one point each, its walk
+/// starting from the nearest earlier inserted vertex of its set.
+__global__ void k_setup_list(Workers W, const int* __restrict__ list, int n, const int32_t* __restrict__ vset,
+                             const int32_t* __restrict__ voff, const int* __restrict__ vert_tet) {
+    const int w = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (w >= n) return;
+    const int v = list[w];
+    const int set = vset[v];
+    W.beg[w] = v;
+    W.end[w] = v + 1;
+    W.pos[w] = 0;
+    W.left[w] = 1;
+    W.nwon[w] = 0;
+    W.parked[w] = 0;
+    W.last[w] = -1;
+    W.wset[w] = set;
+    next_point(W, w);
+    int g = W.skips[set].x;
+    for (int u = v - 1, k = 0; u >= voff[set] && k < 4096; --u, ++k)
+        if (__ldcg(vert_tet + u) >= 0) {
+            g = u;
+            break;
+        }
+    W.guide[w] = g;
+    W.state[w] = WS_DONE;
+}
+
+/// Launches one insertion kernel (0: k_cavity, 1: k_check, 2: k_restar) over
+/// `n` worker slots with G lanes per worker.
+template <int G>
+void launch_insertion_t(int which, const Tables& T, const Workers& W, const Round& R, const double* vx, int n,
+                        cudaStream_t s) {
+    const unsigned grid = unsigned((int64_t(n) * G + 127) / 128);
+    if (which == 0) k_cavity<G><<<grid, 128, 0, s>>>(T, W, R, vx, 0);
+    else if (which == 1) k_check<G><<<grid, 128, 0, s>>>(T, W, R, 0);
+    else k_restar<G><<<grid, 128, 0, s>>>(T, W, R, 0);
+}
+
+void launch_insertion(int lanes, int which, const Tables& T, const Workers& W, const Round& R, const double* vx,
+                      cudaStream_t s) {
+    switch (lanes) {
+        case 4: launch_insertion_t<4>(which, T, W, R, vx, W.n, s); break;
+        case 8: launch_insertion_t<8>(which, T, W, R, vx, W.n, s); break;
+        case 16: launch_insertion_t<16>(which, T, W, R, vx, W.n, s); break;
+        default: launch_insertion_t<32>(which, T, W, R, vx, W.n, s); break;
+    }
+}
+
 
 /// Lists the parked workers (for the big rounds).
 __global__ void k_collect_parked(Workers W, int* list, int* count) {
@@ -1166,6 +1666,12 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     D3G_TRY(tet_count.alloc(1, s));
     D3G_CUDA(cudaMemsetAsync(claim.p, 0xFF, sizeof(unsigned long long) * size_t(T.cap), s));
     D3G_CUDA(cudaMemsetAsync(alive.p, 0, size_t(T.cap), s));
+    // Every slot holds in-range indices from the start (the asynchronous walk
+    // may read a slot before its tet is written), and a vertex not inserted yet
+    // has no tet.
+    D3G_CUDA(cudaMemsetAsync(tv.p, 0, sizeof(int4) * size_t(T.cap), s));
+    D3G_CUDA(cudaMemsetAsync(tn.p, 0, sizeof(int4) * size_t(T.cap), s));
+    D3G_CUDA(cudaMemsetAsync(vert_tet.p, 0xFF, sizeof(int) * size_t(nv), s));
     T.tv = tv.p;
     T.tn = tn.p;
     T.claim = claim.p;
@@ -1319,6 +1825,21 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     Rd.status = status.p;
     const int max_rounds = opt.max_rounds > 0 ? opt.max_rounds : (1 << 20);
     int round = 0;
+    // Asynchronous passes (see k_insert_async): a persistent grid of at most
+    // kAsyncWarps warps per level; the rounds finish what it leaves.
+    const bool use_async = opt.schedule != 1 && !grow;
+    constexpr int kAsyncWarps = kNumSMs * 32;
+    DevBuf<int> alock, anext, aleft, anleft;
+    DevBuf<unsigned long long> astats;
+    if (use_async) {
+        D3G_TRY(alock.alloc(size_t(T.cap), s));
+        D3G_TRY(anext.alloc(1, s));
+        D3G_TRY(aleft.alloc(size_t(nv), s));
+        D3G_TRY(anleft.alloc(1, s));
+        D3G_TRY(astats.alloc(2, s));
+        D3G_CUDA(cudaMemsetAsync(alock.p, 0, sizeof(int) * size_t(T.cap), s));
+        D3G_CUDA(cudaMemsetAsync(astats.p, 0, 2 * sizeof(unsigned long long), s));
+    }
     const bool trace = getenv("D3G_TRACE") != nullptr;
     cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};
     if (opt.timing)
@@ -1357,7 +1878,6 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             WB.st_n = bsn.p;
             WB.cav_cap = kBigCav;
             WB.fac_cap = kBigFac;
-            const unsigned gb = unsigned((int64_t(WB.n) * 32 + 127) / 128);
             for (;;) {
                 if (++round > max_rounds) {
                     set_error("d3g_build: insertion round limit reached");
@@ -1366,9 +1886,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 unsigned long long before = 0;
                 D3G_CUDA(cudaMemcpyAsync(&before, totals.p, sizeof before, cudaMemcpyDeviceToHost, s));
                 k_round_begin<<<1, 1, 0, s>>>(Rd);
-                k_cavity<<<gb, 128, 0, s>>>(T, WB, Rd, vx.p, 0);
-                k_check<<<gb, 128, 0, s>>>(T, WB, Rd, 0);
-                k_restar<<<gb, 128, 0, s>>>(T, WB, Rd, 0);
+                launch_insertion(32, 0, T, WB, Rd, vx.p, s);
+                launch_insertion(32, 1, T, WB, Rd, vx.p, s);
+                launch_insertion(32, 2, T, WB, Rd, vx.p, s);
                 k_round_end<<<1, 1, 0, s>>>(Rd);
                 unsigned long long ht[6];
                 uint32_t hs = 0;
@@ -1425,15 +1945,15 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         D3G_TRY(ddesc.alloc(descs.size(), s));
         D3G_CUDA(cudaMemcpyAsync(ddesc.p, descs.data(), sizeof(LevelDesc) * descs.size(), cudaMemcpyHostToDevice, s));
         k_setup_level<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, ddesc.p, int(descs.size()));
-        unsigned g = unsigned((int64_t(W.n) * 32 + 127) / 128);
+        int lanes = opt.lanes > 0 ? opt.lanes : 32;
         auto one_round = [&](bool timed) {
             k_round_begin<<<1, 1, 0, s>>>(Rd);
             if (timed) cudaEventRecord(kev[0], s);
-            k_cavity<<<g, 128, 0, s>>>(T, W, Rd, vx.p, 0);
+            launch_insertion(lanes, 0, T, W, Rd, vx.p, s);
             if (timed) cudaEventRecord(kev[1], s);
-            k_check<<<g, 128, 0, s>>>(T, W, Rd, 0);
+            launch_insertion(lanes, 1, T, W, Rd, vx.p, s);
             if (timed) cudaEventRecord(kev[2], s);
-            k_restar<<<g, 128, 0, s>>>(T, W, Rd, 0);
+            launch_insertion(lanes, 2, T, W, Rd, vx.p, s);
             if (timed) cudaEventRecord(kev[3], s);
             k_round_end<<<1, 1, 0, s>>>(Rd);
         };
@@ -1463,6 +1983,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             }
             return D3G_OK;
         };
+        auto run_rounds = [&]() -> int {
         D3G_TRY(capture());
         for (;;) {
             const int batch = opt.timing ? 1 : kRoundsPerBatch;
@@ -1491,7 +2012,6 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 // The pool grew: the next batches serve the new workers too.
                 W.n = hn;
                 k_set_int<<<1, 1, 0, s>>>(nworkers.p, W.n);
-                g = unsigned((int64_t(W.n) * 32 + 127) / 128);
                 D3G_TRY(capture());
             }
             if (hs != 0) {
@@ -1521,13 +2041,57 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             // kBigSlots at a time, each until its point is in.
             D3G_TRY(big_rounds());
         }
+        return D3G_OK;
+        };
+        long long async_left = -1;
+        if (use_async) {
+            // The chunks go out in a scattered order (stride coprime with the
+            // chunk count, near the golden ratio of it), so that chunks taken
+            // at the same time lie far apart along the curve.
+            int64_t stride = std::max<int64_t>(1, int64_t(double(W.n) * 0.6180339887));
+            while (std::gcd(stride, int64_t(W.n)) != 1) ++stride;
+            D3G_CUDA(cudaMemsetAsync(anext.p, 0, sizeof(int), s));
+            D3G_CUDA(cudaMemsetAsync(anleft.p, 0, sizeof(int), s));
+            AsyncCtx A{alock.p, anext.p, aleft.p, anleft.p, stride, astats.p};
+            const int warps = std::min(W.n, kAsyncWarps);
+            k_insert_async<<<unsigned((int64_t(warps) * 32 + 127) / 128), 128, 0, s>>>(T, W, A, Rd, vx.p,
+                                                                                      warps);
+            D3G_CUDA(cudaGetLastError());
+            int nleft = 0;
+            uint32_t hs = 0;
+            D3G_CUDA(cudaMemcpyAsync(&nleft, anleft.p, sizeof nleft, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaStreamSynchronize(s));
+            if (hs != 0) {
+                const int st = status_from_bits(hs);
+                if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");
+                return st;
+            }
+            async_left = nleft;
+            // What the pass left goes through the rounds, maxw points at a time.
+            for (int off = 0; off < nleft; off += maxw) {
+                W.n = std::min(maxw, nleft - off);
+                k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, aleft.p + off, W.n, vset.p, voff.p,
+                                                                        T.vert_tet);
+                D3G_TRY(run_rounds());
+            }
+        } else {
+            D3G_TRY(run_rounds());
+        }
         if (trace) {
             cudaEventRecord(ev1, s);
             cudaEventSynchronize(ev1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev0, ev1);
-            fprintf(stderr, "d3g level %d sets %zu workers %d rounds %d inserted %lld attempts %lld ms %.2f\n",
-                    lev, descs.size(), W.n, round - round0, won, attempts, ms);
+            {
+                unsigned long long ht1[2];
+                cudaMemcpy(ht1, totals.p, sizeof ht1, cudaMemcpyDeviceToHost);
+                won = (long long)ht1[0] - won_before;
+                attempts = (long long)ht1[1] - att_before;
+            }
+            fprintf(stderr, "d3g level %d sets %zu workers %d rounds %d inserted %lld attempts %lld "
+                    "left-by-async %lld ms %.2f\n",
+                    lev, descs.size(), W.n, round - round0, won, attempts, async_left, ms);
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
         }
@@ -1652,6 +2216,8 @@ void d3g_options_default(d3g_options* o) {
     o->max_rounds = 0;
     o->timing = 0;
     o->alpha_small = 24;
+    o->lanes = 0;
+    o->schedule = 0;
     o->split = 0;
 }
 

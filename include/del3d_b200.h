@@ -158,6 +158,10 @@ typedef struct d3g_options {
                              /* default 24                                       */
     int32_t split;           /* grow the worker pool within a level as points go */
                              /* in (0 = off)                                     */
+    int32_t lanes;           /* lanes per worker in the lockstep insertion       */
+                             /* kernels: 32, 16, 8 or 4; 0 = 32 (default)        */
+    int32_t schedule;        /* 0 = asynchronous insertion with rounds for what  */
+                             /* it leaves (default); 1 = lockstep rounds only    */
 } d3g_options;
 
 /* What a build did (filled by d3g_build and d3g_build_device). */
