@@ -74,6 +74,10 @@ def parse_args():
                          "(--n uniform points); predicates / sort: the predicate and "
                          "spatial-sort microbenchmarks, one line each")
     ap.add_argument("--n", type=int, default=PLAIN_N, help="points of the plain workload")
+    ap.add_argument("--dist", default="uniform", choices=["uniform", "clusters", "lattice", "sphere"],
+                    help="distribution of the plain workload")
+    ap.add_argument("--schedule", type=int, default=0,
+                    help="0: asynchronous insertion (default); 1: lockstep rounds only")
     ap.add_argument("--timing", action="store_true",
                     help="plain workload: launch each round's kernels separately with event "
                          "timing (the form the ncu launch list captures)")
@@ -733,7 +737,7 @@ def run_predicates(args):
 
 
 def run_plain(args):
-    """One plain single-set build of --n uniform points per step (mt19937 seed 6)."""
+    """One plain single-set build of --n points of --dist per step (mt19937 seed 6)."""
     import torch
 
     import del3d_b200 as d3
@@ -741,25 +745,28 @@ def run_plain(args):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
-    x = torch.from_numpy(d3.gen_uniform(args.n, PLAIN_SEED)).to(dev)
-    out = torch.empty((8 * args.n + 64, 4), dtype=torch.int32, device=dev)
+    x = torch.from_numpy(d3.gen_set(args.dist, args.n, PLAIN_SEED)).to(dev)
+    n = x.shape[0]
+    out = torch.empty((8 * n + 64, 4), dtype=torch.int32, device=dev)
     stats = {}
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            d3.build_device(x, out=out, stream=stream.cuda_stream, timing=args.timing)
+            d3.build_device(x, out=out, stream=stream.cuda_stream, timing=args.timing,
+                            schedule=args.schedule)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
             cells, _ = d3.build_device(x, out=out, stream=stream.cuda_stream, timing=args.timing,
-                                       stats=stats)
+                                       stats=stats, schedule=args.schedule)
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    print(json.dumps({"metric": "plain single-set build points/s", "value": args.n / (ms / 1000.0),
+    print(json.dumps({"metric": "plain single-set build points/s", "value": n / (ms / 1000.0),
                       "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                       "ms_per_step": ms, "timing": bool(args.timing), "cells": int(cells.shape[0]),
-                      "config": {"workload": f"{args.n} points uniform in [0,1)^3 (mt19937 seed {PLAIN_SEED})"},
+                      "config": {"workload": f"{n} points, {args.dist} (seed {PLAIN_SEED})",
+                                 "schedule": "rounds" if args.schedule == 1 else "asynchronous"},
                       "build_stats": {k: (round(v, 3) if isinstance(v, float) else v)
                                       for k, v in stats.items()}}))
     return 0

@@ -113,6 +113,7 @@ struct Workers {
     int4* st_n;   // ... and neighbours
     int* wset;        // set of each worker
     const int4* skips; // per set: its first tet's vertices (inserted before the rounds)
+    const uint8_t* set_exact;  // per set: 1 if its coordinates make the filters exact
     int cav_cap;
     int fac_cap;
     int n;
@@ -156,18 +157,20 @@ __global__ void k_round_end(Round R) {
     R.totals[5] = (unsigned long long)active;
 }
 
-/// orient3d of tet (q0,q1,q2,q3) with vertex i replaced by p.
-__device__ __forceinline__ int orient_replaced(const Pt* q, int i, const Pt& p, uint32_t* st) {
-    switch (i) {
-        case 0: return orient3d(p, q[1], q[2], q[3], st);
-        case 1: return orient3d(q[0], p, q[2], q[3], st);
-        case 2: return orient3d(q[0], q[1], p, q[3], st);
-        default: return orient3d(q[0], q[1], q[2], p, st);
-    }
+/// orient3d of tet (q0,q1,q2,q3) with vertex i replaced by p (one call site);
+/// `ex`: the set's coordinates make the filter exact.
+__device__ __forceinline__ int orient_replaced(const Pt* q, int i, const Pt& p, bool ex, uint32_t* st) {
+    const Pt& A = i == 0 ? p : q[0];
+    const Pt& B = i == 1 ? p : q[1];
+    const Pt& C = i == 2 ? p : q[2];
+    const Pt& D = i == 3 ? p : q[3];
+    return orient3d_x(A, B, C, D, ex, st);
 }
 
-/// The reference's conflict test, src/triangulation.cpp:588-602.
-__device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __restrict__ vx,
+/// The reference's conflict test, src/triangulation.cpp:588-602.  `ex`: the
+/// point set's coordinates span few enough bits that the orient3d and in_sphere
+/// filters compute their determinants exactly.
+__device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __restrict__ vx, bool ex,
                             uint32_t* st) {
     const int ip = inf_pos(t);
     if (ip >= 0) {
@@ -178,13 +181,19 @@ __device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __
         const int o2 = ip == 0 ? 3 : (ip == 1 ? 0 : (ip == 2 ? 3 : 2));
         const int va = at(t, o0), vb = at(t, o1), vd = at(t, o2);
         const Pt a = vpt(vx, va), b = vpt(vx, vb), d = vpt(vx, vd);
-        const int s = orient3d(a, b, d, p, st);
+        const int s = orient3d_x(a, b, d, p, ex, st);
         if (s != 0) return s > 0;
         const int64_t id[4] = {va, vb, vd, pid};
         return coplanar_in_circle(a, b, d, p, id, st) > 0;
     }
-    const int64_t id[5] = {t.x, t.y, t.z, t.w, pid};
-    return in_sphere(vpt(vx, t.x), vpt(vx, t.y), vpt(vx, t.z), vpt(vx, t.w), p, id, st) > 0;
+    const Pt a = vpt(vx, t.x), b = vpt(vx, t.y), c = vpt(vx, t.z), d = vpt(vx, t.w);
+    const InSphereFilter f = in_sphere_filter(a, b, c, d, p);
+    if (f.certain || (ex && f.det != 0.0)) return f.det < 0.0;   // in_sphere = -sign(det)
+    if (ex)
+        return in_sphere_tiebreak_exact(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, p.x, p.y, p.z,
+                                        t.x, t.y, t.z, t.w, pid, st) > 0;
+    return in_sphere_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, p.x, p.y, p.z, t.x,
+                                t.y, t.z, t.w, pid, f.det, 1, st) > 0;
 }
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -245,7 +254,7 @@ struct Lanes {
 /// -1 for a group that is not live or hit the walk limit.
 template <int G>
 __device__ int walk_g(bool live, int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
-                      uint32_t* st, const Lanes<G>& L, int* nsteps) {
+                      bool ex, uint32_t* st, const Lanes<G>& L, int* nsteps) {
     int4 tv = make_int4(0, 0, 0, 0);
     if (live) {
         tv = T.tv[t];
@@ -266,7 +275,7 @@ __device__ int walk_g(bool live, int t, const Pt& p, int pid, const Tables& T, c
             h = h * 1664525u + 1013904223u;
             if (L.sub < 4 && (at(tn, L.sub) >> 2) != prev) {
                 const Pt q[4] = {vpt(vx, tv.x), vpt(vx, tv.y), vpt(vx, tv.z), vpt(vx, tv.w)};
-                neg = orient_replaced(q, L.sub, p, st) < 0;
+                neg = orient_replaced(q, L.sub, p, ex, st) < 0;
             }
         }
         const unsigned m = L.own(__ballot_sync(kFull, neg)) & 0xFu;
@@ -320,10 +329,11 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
     }
     if (!__any_sync(kFull, live)) return;
     const Pt p = live ? vpt(vx, v) : Pt{0.0, 0.0, 0.0};
+    const bool ex = live && W.set_exact[W.wset[w]] != 0;
     int start = 0;
     if (live) start = T.vert_tet[W.last[w] >= 0 ? W.last[w] : W.guide[w]];
     int wsteps = 0;
-    const int seed = walk_g<G>(live, start, p, v, T, vx, R.status, L, &wsteps);
+    const int seed = walk_g<G>(live, start, p, v, T, vx, ex, R.status, L, &wsteps);
     if (R.steps && live && L.sub == 0) atomicAdd(R.steps, (unsigned long long)wsteps);
     if (live && seed < 0) {
         if (L.sub == 0) W.state[w] = WS_FAIL;
@@ -366,7 +376,7 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
                 kind = 3;                               // seen by us: decided below
             } else if ((old >> 1) < mine) {
                 abort = true;                           // an earlier point holds it
-            } else if (in_conflict(T.tv[nb], p, v, vx, R.status)) {
+            } else if (in_conflict(T.tv[nb], p, v, vx, ex, R.status)) {
                 const unsigned long long o2 = atomicMin(T.claim + nb, key);
                 if ((o2 >> 1) < mine) abort = true;
                 else kind = 2;
@@ -621,7 +631,8 @@ struct AsyncCtx {
     int* leftover;                  // points left for the rounds
     int* n_leftover;
     int64_t stride;                 // chunk q of the queue is chunk (q * stride) % W.n
-    unsigned long long* stats;      // [0] lock conflicts, [1] walk restarts
+    unsigned long long* stats;      // [0] lock conflicts, [1] walk restarts, [2] invalid seeds,
+                                    // [3] regions too big, [4] points left, [5] first points left
 };
 
 using LockRef = cuda::atomic_ref<int, cuda::thread_scope_device>;
@@ -646,7 +657,7 @@ __device__ __forceinline__ int4 ld4(const int4* p) { return __ldcg(p); }
 /// be stale, so the tet it returns is only a candidate, checked under its lock.
 /// Returns -1 after kAsyncWalkLimit steps.
 __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
-                          uint32_t* st, int lane) {
+                          bool ex, uint32_t* st, int lane) {
     int4 tv = ld4(T.tv + t);
     {
         const int ip = inf_pos(tv);
@@ -665,7 +676,7 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
         if (lane < 4 && (at(tn, lane) >> 2) != prev && tv.x != kInf && tv.y != kInf && tv.z != kInf &&
             tv.w != kInf) {
             const Pt q[4] = {vpt(vx, tv.x), vpt(vx, tv.y), vpt(vx, tv.z), vpt(vx, tv.w)};
-            neg = orient_replaced(q, lane, p, st) < 0;
+            neg = orient_replaced(q, lane, p, ex, st) < 0;
         }
         const unsigned m = __ballot_sync(kFull, neg) & 0xFu;
         if (m == 0) return t;
@@ -716,12 +727,12 @@ enum : int { AI_DONE = 0, AI_RETRY = 1, AI_LEAVE = 2 };
 /// AI_DONE: inserted; AI_RETRY: a lock was taken by another warp (nothing
 /// changed, every lock given back); AI_LEAVE: leave it for the rounds.
 __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, const AsyncCtx& A,
-                            const double* __restrict__ vx, uint32_t* st, int slot, int lane,
+                            const double* __restrict__ vx, bool ex, uint32_t* st, int slot, int lane,
                             unsigned long long* nC, unsigned long long* nF) {
     const int owner = slot + 1;
     const int region = owner << 1, ring = region | 1;
     const Pt p = vpt(vx, v);
-    const int seed = walk_async(t0, p, v, T, vx, st, lane);
+    const int seed = walk_async(t0, p, v, T, vx, ex, st, lane);
     if (seed < 0) {
         if (lane == 0) atomicAdd(A.stats + 1, 1ull);
         return AI_RETRY;
@@ -734,7 +745,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         int seen = 0;
         if (!try_lock(A.lock, seed, region, &seen)) {
             res = 1;
-        } else if (!__ldcg(T.alive + seed) || !in_conflict(ld4(T.tv + seed), p, v, vx, st)) {
+        } else if (!__ldcg(T.alive + seed) || !in_conflict(ld4(T.tv + seed), p, v, vx, ex, st)) {
             unlock_if(A.lock, seed, region);
             res = 2;
         } else {
@@ -743,7 +754,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
     }
     res = __shfl_sync(kFull, res, 0);
     if (res != 0) {
-        if (res == 1 && lane == 0) atomicAdd(A.stats, 1ull);
+        if (lane == 0) atomicAdd(A.stats + (res == 1 ? 0 : 2), 1ull);
         return AI_RETRY;
     }
     __syncwarp();
@@ -762,7 +773,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             int seen = 0;
             if (try_lock(A.lock, nb, ring, &seen)) {
                 got = nb;
-                if (in_conflict(ld4(T.tv + nb), p, v, vx, st)) {
+                if (in_conflict(ld4(T.tv + nb), p, v, vx, ex, st)) {
                     LockRef(A.lock[nb]).store(region, cuda::memory_order_relaxed);
                     kind = 2;
                 } else {
@@ -792,7 +803,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             }
             __syncwarp();
             for (int k = lane; k < ncav; k += 32) unlock_if(A.lock, cav[k], region);
-            if (lane == 0 && ab) atomicAdd(A.stats, 1ull);
+            if (lane == 0) atomicAdd(A.stats + (ab ? 0 : 3), 1ull);
             outcome = ab ? AI_RETRY : AI_LEAVE;
             break;
         }
@@ -919,6 +930,7 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
         const int w = int((int64_t(q) * A.stride) % W.n);
         const int b = W.beg[w], len = W.end[w] - b;
         const int4 sk = W.skips[W.wset[w]];
+        const bool ex = W.set_exact[W.wset[w]] != 0;
         int pos = W.pos[w], left = W.left[w];
         int v = W.cur[w];
         int last = -1;
@@ -928,7 +940,7 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
             for (int attempt = 0; attempt < kAsyncRetries && outcome == AI_RETRY; ++attempt) {
                 if (attempt > 0) __nanosleep(200u << min(attempt, 6));
                 const int t0 = __ldcg(T.vert_tet + (last >= 0 ? last : guide));
-                outcome = insert_async(v, t0, T, W, A, vx, R.status, slot, lane, &nC, &nF);
+                outcome = insert_async(v, t0, T, W, A, vx, ex, R.status, slot, lane, &nC, &nF);
                 ++tries;
                 if (__ldcg(R.status) != 0) outcome = AI_LEAVE;
             }
@@ -937,6 +949,8 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
                 last = v;
             } else if (lane == 0) {
                 A.leftover[atomicAdd(A.n_leftover, 1)] = v;
+                atomicAdd(A.stats + 4, 1ull);
+                if (last < 0) atomicAdd(A.stats + 5, 1ull);
             }
             if (__ldcg(R.status) != 0) break;
             // next point of the chunk (as next_point)
@@ -986,6 +1000,43 @@ __global__ void k_setup_list(Workers W, const int* __restrict__ list, int n, con
         }
     W.guide[w] = g;
     W.state[w] = WS_DONE;
+}
+
+/// Per set, the exponent span of its vertex coordinates (Span: lowest set bit,
+/// just above the highest), reduced over runs of vertices of one set.
+__global__ void k_set_span(const double* __restrict__ vx, int nv, const int32_t* __restrict__ vset,
+                           int* __restrict__ smin, int* __restrict__ stop) {
+    constexpr int kRun = 64;
+    const int64_t first = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * kRun;
+    if (first >= nv) return;
+    const int last = int(min(int64_t(nv), first + kRun));
+    int set = vset[first];
+    Span sp;
+    for (int v = int(first); v <= last; ++v) {
+        if (v == last || vset[v] != set) {
+            if (!sp.empty()) {
+                atomicMin(smin + set, sp.emin);
+                atomicMax(stop + set, sp.top);
+            }
+            if (v == last) break;
+            set = vset[v];
+            sp = Span();
+        }
+        sp.add(vx[3 * int64_t(v)]);
+        sp.add(vx[3 * int64_t(v) + 1]);
+        sp.add(vx[3 * int64_t(v) + 2]);
+    }
+}
+
+/// A set whose span makes the orient3d and in_sphere filters exact.
+__global__ void k_set_exact(const int* __restrict__ smin, const int* __restrict__ stop, int nsets,
+                            uint8_t* __restrict__ ex) {
+    const int s = int(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= nsets) return;
+    Span sp;
+    sp.emin = smin[s];
+    sp.top = stop[s];
+    ex[s] = (sp.exact_in_double(5, 7) && sp.exact_in_double(3, 3)) ? 1 : 0;
 }
 
 /// Launches one insertion kernel (0: k_cavity, 1: k_check, 2: k_restar) over
@@ -1681,6 +1732,25 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     T.tet_count = tet_count.p;
     k_set_int<<<1, 1, 0, s>>>(tet_count.p, 5 * nsets);
     k_init_tets<<<grid_for(nsets, 64), 64, 0, s>>>(T, vx.p, skips.p, nsets, status.p);
+    // Sets whose coordinates span few bits (integer lattices, coarse grids):
+    // their filters are exact, so their degenerate queries skip the exact stage.
+    DevBuf<int> set_span;
+    DevBuf<uint8_t> set_exact;
+    D3G_TRY(set_span.alloc(size_t(2) * size_t(nsets), s));
+    D3G_TRY(set_exact.alloc(size_t(nsets), s));
+    {
+        std::vector<int> init(size_t(2) * size_t(nsets));
+        for (int i = 0; i < nsets; ++i) {
+            init[size_t(i)] = 1 << 20;                   // emin of an empty span
+            init[size_t(nsets) + size_t(i)] = -(1 << 20); // top of an empty span
+        }
+        D3G_CUDA(cudaMemcpyAsync(set_span.p, init.data(), sizeof(int) * init.size(), cudaMemcpyHostToDevice, s));
+        if (nv > 0)
+            k_set_span<<<grid_for((int64_t(nv) + 63) / 64, 128, 1 << 30), 128, 0, s>>>(vx.p, nv, vset.p, set_span.p,
+                                                                                 set_span.p + nsets);
+        k_set_exact<<<grid_for(nsets, 128), 128, 0, s>>>(set_span.p, set_span.p + nsets, nsets, set_exact.p);
+        D3G_CUDA(cudaStreamSynchronize(s));   // `init` must outlive the copy
+    }
 
     // ---- workers ----
     // A level of s points goes into a triangulation of p earlier points.  Two
@@ -1803,6 +1873,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     W.parked = wparked.p;
     W.wset = wset.p;
     W.skips = skips.p;
+    W.set_exact = set_exact.p;
     W.pos = wpos.p;
     W.left = wleft.p;
     W.nwon = wnwon.p;
@@ -1836,9 +1907,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         D3G_TRY(anext.alloc(1, s));
         D3G_TRY(aleft.alloc(size_t(nv), s));
         D3G_TRY(anleft.alloc(1, s));
-        D3G_TRY(astats.alloc(2, s));
+        D3G_TRY(astats.alloc(6, s));
         D3G_CUDA(cudaMemsetAsync(alock.p, 0, sizeof(int) * size_t(T.cap), s));
-        D3G_CUDA(cudaMemsetAsync(astats.p, 0, 2 * sizeof(unsigned long long), s));
+        D3G_CUDA(cudaMemsetAsync(astats.p, 0, 6 * sizeof(unsigned long long), s));
     }
     const bool trace = getenv("D3G_TRACE") != nullptr;
     cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -2089,9 +2160,13 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 won = (long long)ht1[0] - won_before;
                 attempts = (long long)ht1[1] - att_before;
             }
+            unsigned long long as[6] = {0, 0, 0, 0, 0, 0};
+            if (use_async) cudaMemcpy(as, astats.p, sizeof as, cudaMemcpyDeviceToHost);
             fprintf(stderr, "d3g level %d sets %zu workers %d rounds %d inserted %lld attempts %lld "
-                    "left-by-async %lld ms %.2f\n",
-                    lev, descs.size(), W.n, round - round0, won, attempts, async_left, ms);
+                    "left-by-async %lld ms %.2f | async totals: lock-conflicts %llu walk-restarts %llu "
+                    "bad-seeds %llu too-big %llu left %llu first-left %llu\n",
+                    lev, descs.size(), W.n, round - round0, won, attempts, async_left, ms, as[0], as[1],
+                    as[2], as[3], as[4], as[5]);
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
         }

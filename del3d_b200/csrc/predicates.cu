@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(128) k_exact_in_sphere(const double* __restric
         const Pt a = load_pt(pts, t[0]), b = load_pt(pts, t[1]), c = load_pt(pts, t[2]),
                  d = load_pt(pts, t[3]), e = load_pt(pts, t[4]);
         const InSphereFilter f = in_sphere_filter(a, b, c, d, e);
-        int s = in_sphere_exact(a, b, c, d, e, f.det, status);
-        if (s == 0 && perturbed) s = in_sphere_perturb(a, b, c, d, e, id, status);
+        const int s = in_sphere_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, e.x, e.y,
+                                           e.z, id[0], id[1], id[2], id[3], id[4], f.det, perturbed, status);
         out[q] = int8_t(s);
     }
 }
@@ -156,11 +156,9 @@ __global__ void __launch_bounds__(128) k_coplanar(const double* __restrict__ pts
                     s = sign_of(f.det);
                 } else {
                     atomicAdd(nexact, 1ull);
-                    s = in_circle_exact(p0, p1, p2, p3, f.det, status);
-                    if (s == 0 && kind == D3G_COPLANAR_IN_CIRCLE) {
-                        const int64_t id[4] = {t[0], t[1], t[2], t[3]};
-                        s = in_circle_perturb(p0, p1, p2, p3, id, status);
-                    }
+                    s = in_circle_degenerate(p0.x, p0.y, p0.z, p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y,
+                                             p3.z, t[0], t[1], t[2], t[3], f.det,
+                                             kind == D3G_COPLANAR_IN_CIRCLE ? 1 : 0, status);
                 }
             }
         }

@@ -133,13 +133,19 @@ D3G_HD int orient3d_num(const Pt& a, const Pt& b, const Pt& c, const Pt& d, cons
     return -num_sign(det);
 }
 
-/// Exact orient3d for a call the filter left uncertain; `fdet` is the filter's
-/// value (exact whenever the exponent span is small).
-D3G_NOINLINE int orient3d_exact(const Pt& a, const Pt& b, const Pt& c, const Pt& d, double fdet,
-                                uint32_t* status) {
+/// Exact orient3d of a call the filter left uncertain.  Out of line and shared
+/// by every call site (one copy of the degenerate-case code keeps the kernels'
+/// instruction footprint small when many lanes take it), with scalar arguments
+/// so that nothing needs an address in local memory.  `fdet` is the filter's
+/// value, exact - and used - when the exponent span is small (integer lattices,
+/// coarse grids); otherwise fixed-width integers.
+D3G_NOINLINE int orient3d_degenerate(double ax, double ay, double az, double bx, double by, double bz,
+                                     double cx, double cy, double cz, double dx, double dy, double dz,
+                                     double fdet, uint32_t* status) {
+    const Pt a{ax, ay, az}, b{bx, by, bz}, c{cx, cy, cz}, d{dx, dy, dz};
     Span s;
-    s.add(a.x); s.add(a.y); s.add(a.z); s.add(b.x); s.add(b.y); s.add(b.z);
-    s.add(c.x); s.add(c.y); s.add(c.z); s.add(d.x); s.add(d.y); s.add(d.z);
+    s.add(ax); s.add(ay); s.add(az); s.add(bx); s.add(by); s.add(bz);
+    s.add(cx); s.add(cy); s.add(cz); s.add(dx); s.add(dy); s.add(dz);
     if (s.exact_in_double(3, 3)) return -sign_of(fdet);
     const int L = limbs_for(3 * (s.bits() + 1) + 3);
     if (L <= 2) return orient3d_num<WideS<2>>(a, b, c, d, NumFrom<WideS<2>>{s.emin});
@@ -149,9 +155,22 @@ D3G_NOINLINE int orient3d_exact(const Pt& a, const Pt& b, const Pt& c, const Pt&
     return 0;
 }
 
+D3G_HD int orient3d_exact(const Pt& a, const Pt& b, const Pt& c, const Pt& d, double fdet, uint32_t* status) {
+    return orient3d_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, fdet, status);
+}
+
 D3G_HD int orient3d(const Pt& a, const Pt& b, const Pt& c, const Pt& d, uint32_t* status) {
     const Orient3dFilter f = orient3d_filter(a, b, c, d);
     if (f.certain) return -sign_of(f.det);
+    return orient3d_exact(a, b, c, d, f.det, status);
+}
+
+/// orient3d where the caller knows the filter's arithmetic is exact for these
+/// points when `exact` is set (a point set whose coordinates span few bits):
+/// then the filter value is the determinant and no exact stage is needed.
+D3G_HD int orient3d_x(const Pt& a, const Pt& b, const Pt& c, const Pt& d, bool exact, uint32_t* status) {
+    const Orient3dFilter f = orient3d_filter(a, b, c, d);
+    if (f.certain || exact) return -sign_of(f.det);
     return orient3d_exact(a, b, c, d, f.det, status);
 }
 
@@ -251,19 +270,15 @@ D3G_HD int in_sphere_num(const Pt& a, const Pt& b, const Pt& c, const Pt& d, con
     return -num_sign(det);
 }
 
-D3G_NOINLINE int in_sphere_exact(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e,
-                                 double fdet, uint32_t* status) {
-    Span s;
-    s.add(a.x); s.add(a.y); s.add(a.z); s.add(b.x); s.add(b.y); s.add(b.z);
-    s.add(c.x); s.add(c.y); s.add(c.z); s.add(d.x); s.add(d.y); s.add(d.z);
-    s.add(e.x); s.add(e.y); s.add(e.z);
-    if (s.exact_in_double(5, 7)) return -sign_of(fdet);
-    const int L = limbs_for(5 * (s.bits() + 1) + 7);
-    if (L <= 2) return in_sphere_num<WideS<2>>(a, b, c, d, e, NumFrom<WideS<2>>{s.emin});
-    if (L <= 4) return in_sphere_num<WideS<4>>(a, b, c, d, e, NumFrom<WideS<4>>{s.emin});
-    if (L <= kMaxLimbs) return in_sphere_num<WideV>(a, b, c, d, e, NumFrom<WideV>{s.emin, L});
-    report(status, ST_EXACT_CAPACITY);
-    return 0;
+D3G_NOINLINE int in_sphere_degenerate(double ax, double ay, double az, double bx, double by, double bz,
+                                      double cx, double cy, double cz, double dx, double dy, double dz,
+                                      double ex, double ey, double ez, int64_t id0, int64_t id1, int64_t id2,
+                                      int64_t id3, int64_t id4, double fdet, int perturbed, uint32_t* status);
+
+D3G_HD int in_sphere_exact(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e, double fdet,
+                           uint32_t* status) {
+    return in_sphere_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, e.x, e.y, e.z, 0, 1,
+                                2, 3, 4, fdet, 0, status);
 }
 
 D3G_HD int in_sphere_unperturbed(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e,
@@ -282,38 +297,100 @@ D3G_HD bool lexico_less(const Pt& p, const Pt& q) {
 /// The cospherical tie-break (src/predicates.cpp:211-231).  `id` holds the
 /// identities of a,b,c,d,e; slot order (a,b,c,d,e) is kept among equal points,
 /// as the reference's std::sort of five elements (an insertion sort) keeps it.
-D3G_NOINLINE int in_sphere_perturb(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e,
-                                   const int64_t* id, uint32_t* status) {
-    const Pt* p[5] = {&a, &b, &c, &d, &e};
-    int64_t pid[5] = {id[0], id[1], id[2], id[3], id[4]};
-    for (int i = 1; i < 5; ++i) {
-        const Pt* v = p[i];
-        const int64_t vi = pid[i];
-        int j = i;
-        while (j > 0 && lexico_less(*v, *p[j - 1])) {
-            p[j] = p[j - 1];
-            pid[j] = pid[j - 1];
-            --j;
+/// The slot (0-4) of (a, b, c, d, e) that comes last when the five points are
+/// sorted lexicographically with equal points kept in slot order (a stable
+/// sort, as the reference's insertion-sort std::sort of five elements is),
+/// leaving out slot `skip` (-1: none).  Registers only.
+D3G_HD int lexico_last(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e, int skip) {
+    int best = skip == 0 ? 1 : 0;
+    Pt bp = skip == 0 ? b : a;
+#pragma unroll
+    for (int k = 1; k < 5; ++k) {
+        if (k == skip || k == best) continue;
+        const Pt& q = k == 1 ? b : (k == 2 ? c : (k == 3 ? d : e));
+        if (!lexico_less(q, bp)) {   // a later slot wins ties
+            best = k;
+            bp = q;
         }
-        p[j] = v;
-        pid[j] = vi;
     }
-    for (int i = 4; i > 2; --i) {
-        if (pid[i] == id[4]) return -1;
-        int o;
-        if (pid[i] == id[3] && (o = orient3d(a, b, c, e, status)) != 0) return o;
-        if (pid[i] == id[2] && (o = orient3d(a, b, e, d, status)) != 0) return o;
-        if (pid[i] == id[1] && (o = orient3d(a, e, c, d, status)) != 0) return o;
-        if (pid[i] == id[0] && (o = orient3d(e, b, c, d, status)) != 0) return o;
+    return best;
+}
+
+/// The cospherical tie-break (src/predicates.cpp:211-231): walking down the
+/// lexicographic order from the largest point, the first point that is e
+/// gives NEGATIVE; the first other point whose replacement by e gives a
+/// non-zero orient3d gives that sign.  `id0..id4` are the identities of a..e
+/// (the reference compares pointers, so equal identities are the same point).
+template <bool EX = false>
+D3G_HD int in_sphere_perturb(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e, int64_t id0,
+                             int64_t id1, int64_t id2, int64_t id3, int64_t id4, uint32_t* status) {
+    int skip = -1;
+#pragma unroll 1
+    for (int r = 0; r < 2; ++r) {
+        const int k = lexico_last(a, b, c, d, e, skip);
+        skip = k;
+        const int64_t idk = k == 0 ? id0 : (k == 1 ? id1 : (k == 2 ? id2 : (k == 3 ? id3 : id4)));
+        if (idk == id4) return -1;
+        // The reference tests d, c, b, a in this order; each replaces that slot by e.
+#pragma unroll 1
+        for (int j = 3; j >= 0; --j) {
+            const int64_t idj = j == 0 ? id0 : (j == 1 ? id1 : (j == 2 ? id2 : id3));
+            if (idk != idj) continue;
+            const Pt& A = j == 0 ? e : a;
+            const Pt& B = j == 1 ? e : b;
+            const Pt& C = j == 2 ? e : c;
+            const Pt& D = j == 3 ? e : d;
+            const int o = orient3d_x(A, B, C, D, EX, status);
+            if (o != 0) return o;
+        }
     }
     return -1;
 }
 
+/// Exact sign of in_sphere (and, with `perturbed`, the tie-break) for a call the
+/// filter left uncertain; shared and out of line like orient3d_degenerate.
+D3G_NOINLINE int in_sphere_degenerate(double ax, double ay, double az, double bx, double by, double bz,
+                                      double cx, double cy, double cz, double dx, double dy, double dz,
+                                      double ex, double ey, double ez, int64_t id0, int64_t id1, int64_t id2,
+                                      int64_t id3, int64_t id4, double fdet, int perturbed, uint32_t* status) {
+    const Pt a{ax, ay, az}, b{bx, by, bz}, c{cx, cy, cz}, d{dx, dy, dz}, e{ex, ey, ez};
+    Span s;
+    s.add(ax); s.add(ay); s.add(az); s.add(bx); s.add(by); s.add(bz);
+    s.add(cx); s.add(cy); s.add(cz); s.add(dx); s.add(dy); s.add(dz);
+    s.add(ex); s.add(ey); s.add(ez);
+    int sign;
+    if (s.exact_in_double(5, 7)) {
+        sign = -sign_of(fdet);
+    } else {
+        const int L = limbs_for(5 * (s.bits() + 1) + 7);
+        if (L <= 2) sign = in_sphere_num<WideS<2>>(a, b, c, d, e, NumFrom<WideS<2>>{s.emin});
+        else if (L <= 4) sign = in_sphere_num<WideS<4>>(a, b, c, d, e, NumFrom<WideS<4>>{s.emin});
+        else if (L <= kMaxLimbs) sign = in_sphere_num<WideV>(a, b, c, d, e, NumFrom<WideV>{s.emin, L});
+        else {
+            report(status, ST_EXACT_CAPACITY);
+            return 0;
+        }
+    }
+    if (sign != 0 || !perturbed) return sign;
+    return in_sphere_perturb(a, b, c, d, e, id0, id1, id2, id3, id4, status);
+}
+
+/// The tie-break of an exactly cospherical in_sphere call for points whose
+/// filter arithmetic is exact (shared and out of line).
+D3G_NOINLINE int in_sphere_tiebreak_exact(double ax, double ay, double az, double bx, double by, double bz,
+                                          double cx, double cy, double cz, double dx, double dy, double dz,
+                                          double ex, double ey, double ez, int64_t id0, int64_t id1,
+                                          int64_t id2, int64_t id3, int64_t id4, uint32_t* status) {
+    const Pt a{ax, ay, az}, b{bx, by, bz}, c{cx, cy, cz}, d{dx, dy, dz}, e{ex, ey, ez};
+    return in_sphere_perturb<true>(a, b, c, d, e, id0, id1, id2, id3, id4, status);
+}
+
 D3G_HD int in_sphere(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e,
                      const int64_t* id, uint32_t* status) {
-    const int s = in_sphere_unperturbed(a, b, c, d, e, status);
-    if (s != 0) return s;
-    return in_sphere_perturb(a, b, c, d, e, id, status);
+    const InSphereFilter f = in_sphere_filter(a, b, c, d, e);
+    if (f.certain) return -sign_of(f.det);
+    return in_sphere_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, e.x, e.y, e.z, id[0],
+                                id[1], id[2], id[3], id[4], f.det, 1, status);
 }
 
 // =============================================================================
@@ -460,60 +537,92 @@ D3G_HD int in_circle_num(const Pt& p, const Pt& q, const Pt& r, const Pt& t, con
     return num_sign(det);
 }
 
-D3G_NOINLINE int in_circle_exact(const Pt& p0, const Pt& p1, const Pt& p2, const Pt& p,
-                                 double fdet, uint32_t* status) {
+/// The slot (0-3) of (p0, p1, p2, p) last in lexicographic order with equal
+/// points kept in slot order, among the slots not in `excluded` (bit mask).
+D3G_HD int lexico_last4(const Pt& p0, const Pt& p1, const Pt& p2, const Pt& p, unsigned excluded) {
+    int best = -1;
+    Pt bp = p0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (excluded & (1u << k)) continue;
+        const Pt& q = k == 0 ? p0 : (k == 1 ? p1 : (k == 2 ? p2 : p));
+        if (best < 0 || !lexico_less(q, bp)) {
+            best = k;
+            bp = q;
+        }
+    }
+    return best;
+}
+
+/// The cocircular tie-break (src/predicates2.cpp:241-258): walking down the
+/// lexicographic order of (p0, p1, p2, p) from the largest, the first point
+/// that is p gives NEGATIVE; the first other point whose replacement by p
+/// gives a non-zero coplanar orientation gives it times the orientation of
+/// (p0, p1, p2).  `id0..id3` are the identities of p0, p1, p2, p.
+D3G_HD int in_circle_perturb(const Pt& p0, const Pt& p1, const Pt& p2, const Pt& p, int64_t id0, int64_t id1,
+                             int64_t id2, int64_t id3, uint32_t* status) {
+    const int local = coplanar_orientation3(p0, p1, p2, status);
+    unsigned excluded = 0;
+#pragma unroll 1
+    for (int r = 0; r < 3; ++r) {
+        const int k = lexico_last4(p0, p1, p2, p, excluded);
+        excluded |= 1u << k;
+        const int64_t idk = k == 0 ? id0 : (k == 1 ? id1 : (k == 2 ? id2 : id3));
+        if (idk == id3) return -1;
+#pragma unroll 1
+        for (int j = 2; j >= 0; --j) {
+            const int64_t idj = j == 0 ? id0 : (j == 1 ? id1 : id2);
+            if (idk != idj) continue;
+            const Pt& A = j == 0 ? p : p0;
+            const Pt& B = j == 1 ? p : p1;
+            const Pt& C = j == 2 ? p : p2;
+            const int o = coplanar_orientation3(A, B, C, status);
+            if (o != 0) return o * local;
+        }
+    }
+    return -local;
+}
+
+/// Exact in-circle sign (and, with `perturbed`, the tie-break) for a call the
+/// filter left uncertain; shared and out of line like orient3d_degenerate.
+D3G_NOINLINE int in_circle_degenerate(double ax, double ay, double az, double bx, double by, double bz,
+                                      double cx, double cy, double cz, double px, double py, double pz,
+                                      int64_t id0, int64_t id1, int64_t id2, int64_t id3, double fdet,
+                                      int perturbed, uint32_t* status) {
+    const Pt p0{ax, ay, az}, p1{bx, by, bz}, p2{cx, cy, cz}, p{px, py, pz};
     Span s;
-    s.add(p0.x); s.add(p0.y); s.add(p0.z); s.add(p1.x); s.add(p1.y); s.add(p1.z);
-    s.add(p2.x); s.add(p2.y); s.add(p2.z); s.add(p.x); s.add(p.y); s.add(p.z);
-    if (s.exact_in_double(7, 9)) return sign_of(fdet);
-    const int L = limbs_for(7 * (s.bits() + 1) + 9);
-    if (L <= 4) return in_circle_num<WideS<4>>(p0, p1, p2, p, NumFrom<WideS<4>>{s.emin});
-    if (L <= kMaxLimbs) return in_circle_num<WideV>(p0, p1, p2, p, NumFrom<WideV>{s.emin, L});
-    report(status, ST_EXACT_CAPACITY);
-    return 0;
+    s.add(ax); s.add(ay); s.add(az); s.add(bx); s.add(by); s.add(bz);
+    s.add(cx); s.add(cy); s.add(cz); s.add(px); s.add(py); s.add(pz);
+    int sign;
+    if (s.exact_in_double(7, 9)) {
+        sign = sign_of(fdet);
+    } else {
+        const int L = limbs_for(7 * (s.bits() + 1) + 9);
+        if (L <= 4) sign = in_circle_num<WideS<4>>(p0, p1, p2, p, NumFrom<WideS<4>>{s.emin});
+        else if (L <= kMaxLimbs) sign = in_circle_num<WideV>(p0, p1, p2, p, NumFrom<WideV>{s.emin, L});
+        else {
+            report(status, ST_EXACT_CAPACITY);
+            return 0;
+        }
+    }
+    if (sign != 0 || !perturbed) return sign;
+    return in_circle_perturb(p0, p1, p2, p, id0, id1, id2, id3, status);
 }
 
 D3G_HD int coplanar_in_circle_unperturbed(const Pt& p0, const Pt& p1, const Pt& p2, const Pt& p,
                                           uint32_t* status) {
     const InCircleFilter f = in_circle_filter(p0, p1, p2, p);
     if (f.certain) return sign_of(f.det);
-    return in_circle_exact(p0, p1, p2, p, f.det, status);
-}
-
-/// The cocircular tie-break (src/predicates2.cpp:241-258); id = identities of
-/// p0, p1, p2, p.
-D3G_NOINLINE int in_circle_perturb(const Pt& p0, const Pt& p1, const Pt& p2, const Pt& p,
-                                   const int64_t* id, uint32_t* status) {
-    const Pt* q[4] = {&p0, &p1, &p2, &p};
-    int64_t qid[4] = {id[0], id[1], id[2], id[3]};
-    for (int i = 1; i < 4; ++i) {
-        const Pt* v = q[i];
-        const int64_t vi = qid[i];
-        int j = i;
-        while (j > 0 && lexico_less(*v, *q[j - 1])) {
-            q[j] = q[j - 1];
-            qid[j] = qid[j - 1];
-            --j;
-        }
-        q[j] = v;
-        qid[j] = vi;
-    }
-    const int local = coplanar_orientation3(p0, p1, p2, status);
-    for (int i = 3; i > 0; --i) {
-        if (qid[i] == id[3]) return -1;
-        int o;
-        if (qid[i] == id[2] && (o = coplanar_orientation3(p0, p1, p, status)) != 0) return o * local;
-        if (qid[i] == id[1] && (o = coplanar_orientation3(p0, p, p2, status)) != 0) return o * local;
-        if (qid[i] == id[0] && (o = coplanar_orientation3(p, p1, p2, status)) != 0) return o * local;
-    }
-    return -local;
+    return in_circle_degenerate(p0.x, p0.y, p0.z, p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p.x, p.y, p.z, 0, 1, 2, 3,
+                                f.det, 0, status);
 }
 
 D3G_HD int coplanar_in_circle(const Pt& p0, const Pt& p1, const Pt& p2, const Pt& p,
                               const int64_t* id, uint32_t* status) {
-    const int s = coplanar_in_circle_unperturbed(p0, p1, p2, p, status);
-    if (s != 0) return s;
-    return in_circle_perturb(p0, p1, p2, p, id, status);
+    const InCircleFilter f = in_circle_filter(p0, p1, p2, p);
+    if (f.certain) return sign_of(f.det);
+    return in_circle_degenerate(p0.x, p0.y, p0.z, p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p.x, p.y, p.z, id[0], id[1],
+                                id[2], id[3], f.det, 1, status);
 }
 
 }  // namespace d3g
