@@ -279,19 +279,19 @@ def run_reference(args):
 # ---- ours ----------------------------------------------------------------------------
 
 
-def traffic_per_attempt(kernel):
-    """DRAM bytes per insertion attempt of `kernel` from the committed ncu summary
-    (a line `<kernel> dram bytes per attempt: <number>`), or None."""
+def traffic_per_unit(kernel):
+    """DRAM bytes per unit of work of `kernel` from the committed ncu summary (a line
+    `` `<kernel>` dram bytes per <unit>: <number> ``), as (bytes, unit), or (None, None)."""
     path = os.path.join(ROOT, "profiles", "traffic_per_attempt.md")
     try:
         with open(path) as f:
             for line in f:
-                m = re.search(rf"`{kernel}` dram bytes per attempt: ([0-9.]+)", line)
+                m = re.search(rf"`{kernel}` dram bytes per ([a-z ]+): ([0-9.]+)", line)
                 if m:
-                    return float(m.group(1))
+                    return float(m.group(2)), m.group(1)
     except OSError:
-        return None
-    return None
+        pass
+    return None, None
 
 
 def plain_leg(torch, d3, x, offs, stream, out, sets_idx):
@@ -531,20 +531,34 @@ def run_ours(args):
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
-        # Dominant insertion kernel and its algorithmic bytes: every insertion
-        # reads the vertex record (16 B) and claim word (8 B) of each region and
-        # ring tet, the neighbour record (16 B) of each region tet, and writes
-        # one tet (32 B) per boundary facet.
-        kern = {"k_cavity": stats.get("ms_cavity", 0.0), "k_check": stats.get("ms_check", 0.0),
-                "k_restar": stats.get("ms_restar", 0.0)}
+        # Dominant insertion kernel and its algorithmic bytes (C, F: conflict-
+        # region tets and boundary facets, counted live, split between the
+        # asynchronous passes and the rounds in proportion to the points each
+        # inserted).  An insertion must read the vertex record (16 B) and the
+        # lock or claim word (4 / 8 B) of every region and ring tet and the
+        # neighbour record (16 B) of every region tet; the asynchronous pass
+        # also writes the new tets (32 B each, one per boundary facet) and the
+        # outside tets' back pointers (4 B each).
+        kern = {"k_insert_async": stats.get("ms_async", 0.0), "k_cavity": stats.get("ms_cavity", 0.0),
+                "k_check": stats.get("ms_check", 0.0), "k_restar": stats.get("ms_restar", 0.0)}
         dom = max(kern, key=kern.get)
         C, F = stats.get("region_tets", 0), stats.get("boundary_facets", 0)
-        launches = max(1, stats.get("launches_cavity", 1))
-        bytes_kernel = {"k_cavity": 24 * (C + F) + 16 * C, "k_check": 8 * (C + F) + 16 * F,
-                        "k_restar": 32 * C + 32 * F + 40 * F}[dom]
+        inserted = max(1, n - len(sets))
+        share = min(1.0, stats.get("async_inserted", 0) / inserted)
+        if dom == "k_insert_async":
+            Ca, Fa = C * share, F * share
+            bytes_kernel = 20 * (Ca + Fa) + 16 * Ca + 36 * Fa
+            launches = max(1, stats.get("launches_async", 1))
+        else:
+            Cr, Fr = C * (1 - share), F * (1 - share)
+            bytes_kernel = {"k_cavity": 24 * (Cr + Fr) + 16 * Cr, "k_check": 8 * (Cr + Fr) + 16 * Fr,
+                            "k_restar": 32 * Cr + 32 * Fr + 40 * Fr}[dom]
+            launches = max(1, stats.get("launches_cavity", 1))
         achieved = (bytes_kernel / launches) / (kern[dom] / launches / 1000.0) / 1e9 if kern[dom] else 0.0
-        tpa = traffic_per_attempt(dom)
-        traffic = tpa * stats.get("attempts", 0) / launches if tpa else None
+        per_unit, unit = traffic_per_unit(dom)
+        units = {"inserted point": stats.get("async_inserted", 0),
+                 "attempt": stats.get("attempts", 0) * (1 - share)}.get(unit, 0)
+        traffic = per_unit * units / launches if per_unit else None
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,

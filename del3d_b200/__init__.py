@@ -63,7 +63,8 @@ class BuildStats(ctypes.Structure):
                 ("ms_rounds", ctypes.c_double), ("ms_output", ctypes.c_double),
                 ("ms_cavity", ctypes.c_double), ("ms_check", ctypes.c_double),
                 ("ms_restar", ctypes.c_double), ("launches_cavity", _I64),
-                ("walk_steps", _I64), ("bfs_steps", _I64)]
+                ("walk_steps", _I64), ("bfs_steps", _I64), ("ms_async", ctypes.c_double),
+                ("launches_async", _I64), ("async_inserted", _I64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

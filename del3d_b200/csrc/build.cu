@@ -1899,7 +1899,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     // Asynchronous passes (see k_insert_async): a persistent grid of at most
     // kAsyncWarps warps per level; the rounds finish what it leaves.
     const bool use_async = opt.schedule != 1 && !grow;
-    constexpr int kAsyncWarps = kNumSMs * 32;
+    constexpr int kAsyncWarps = kNumSMs * 32;   // resident at 64 registers a thread
     DevBuf<int> alock, anext, aleft, anleft;
     DevBuf<unsigned long long> astats;
     if (use_async) {
@@ -2125,14 +2125,27 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             D3G_CUDA(cudaMemsetAsync(anleft.p, 0, sizeof(int), s));
             AsyncCtx A{alock.p, anext.p, aleft.p, anleft.p, stride, astats.p};
             const int warps = std::min(W.n, kAsyncWarps);
+            unsigned long long won0 = 0;
+            D3G_CUDA(cudaMemcpyAsync(&won0, totals.p, sizeof won0, cudaMemcpyDeviceToHost, s));
+            if (opt.timing) cudaEventRecord(kev[0], s);
             k_insert_async<<<unsigned((int64_t(warps) * 32 + 127) / 128), 128, 0, s>>>(T, W, A, Rd, vx.p,
                                                                                       warps);
             D3G_CUDA(cudaGetLastError());
+            if (opt.timing) cudaEventRecord(kev[1], s);
             int nleft = 0;
             uint32_t hs = 0;
+            unsigned long long won1 = 0;
             D3G_CUDA(cudaMemcpyAsync(&nleft, anleft.p, sizeof nleft, cudaMemcpyDeviceToHost, s));
             D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaMemcpyAsync(&won1, totals.p, sizeof won1, cudaMemcpyDeviceToHost, s));
             D3G_CUDA(cudaStreamSynchronize(s));
+            R.stats.launches_async += 1;
+            R.stats.async_inserted += int64_t(won1 - won0);
+            if (opt.timing) {
+                float am = 0.f;
+                cudaEventElapsedTime(&am, kev[0], kev[1]);
+                R.stats.ms_async += am;
+            }
             if (hs != 0) {
                 const int st = status_from_bits(hs);
                 if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");

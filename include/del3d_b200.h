@@ -178,6 +178,9 @@ typedef struct d3g_build_stats {
     int64_t launches_cavity;
     int64_t walk_steps;      /* with timing: point-location steps over all attempts  */
     int64_t bfs_steps;       /* with timing: conflict-region growth steps (8 tets each) */
+    double ms_async;         /* with timing: device time of the asynchronous passes  */
+    int64_t launches_async;  /* asynchronous passes (one per level)                  */
+    int64_t async_inserted;  /* points the asynchronous passes inserted              */
 } d3g_build_stats;
 
 typedef struct d3g_result {
