@@ -365,7 +365,7 @@ def serving_leg(torch, d3):
         pinned.append(t.numpy())
     sizes = np.array([a.shape[0] for a in pool])
     out = []
-    with d3.Server(slots=4) as srv:
+    with d3.Server() as srv:
         for t in [srv.submit(pinned[k]) for k in range(8)]:       # warm-up
             srv.wait(t)
         for rate in SERVING_RATES:

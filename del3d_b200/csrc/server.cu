@@ -8,13 +8,14 @@
 // Design
 //   * `slots` worker threads, each with its own non-blocking CUDA stream, so up
 //     to `slots` batches run on the device at once and overlap there.
-//   * A slot that becomes free takes the pending requests in arrival order
-//     (FIFO) for as long as they fit: at most max_batch_sets requests and
+//   * A slot that becomes free takes the request at the head of the queue and,
+//     behind it in arrival order, the requests of a similar size (within a
+//     factor 4) for as long as they fit: at most max_batch_sets requests and
 //     max_batch_points points per batch, and the estimated device memory of
-//     everything in flight within hbm_budget_bytes.  A request that does not
-//     fit waits at the head of the queue (no overtaking, so a large request is
-//     not starved); one larger than the whole budget runs alone once nothing
-//     else is in flight.  Requests that arrive while batches run are admitted
+//     everything in flight within hbm_budget_bytes.  The head is never
+//     overtaken (a large request is not starved; it waits at the head until
+//     memory frees up); one larger than the whole budget runs alone once
+//     nothing else is in flight.  Requests that arrive while batches run are admitted
 //     as soon as a slot and memory free up: the batch is formed when a slot
 //     is free, not when a fixed window closes.
 //   * A batch is one d3g_build_batch-style build (points copied in on the
@@ -47,6 +48,12 @@ constexpr int64_t kBytesPerPoint = 1600;
 constexpr int64_t kBytesPerBatch = int64_t(160) << 20;
 
 int64_t estimate_bytes(int64_t points) { return kBytesPerPoint * points; }
+
+/// Batch formation: requests within a factor kSizeBand of the batch's first
+/// request join it (and any request up to kSmallRequest points joins a batch
+/// of small ones).
+constexpr int64_t kSizeBand = 4;
+constexpr int64_t kSmallRequest = 4096;
 
 struct Request {
     int64_t ticket = 0;
@@ -181,16 +188,25 @@ void worker_main(d3g_server* sv) {
             int64_t pts = 0;
             est = kBytesPerBatch;
             const double t = sv->now();
-            while (!sv->queue.empty()) {
-                Request* r = sv->queue.front();
+            // The head of the queue always goes first (no request is overtaken
+            // for good).  Behind it, only requests of a similar size join its
+            // batch: a batch finishes with its largest set, so a small request
+            // batched with a large one would wait for it.  Others keep their
+            // place for the next free slot.
+            Request* head = sv->queue.front();
+            const int64_t lo = head->n / kSizeBand, hi = std::max<int64_t>(head->n * kSizeBand, kSmallRequest);
+            for (auto it = sv->queue.begin(); it != sv->queue.end();) {
+                Request* r = *it;
                 const int64_t e = estimate_bytes(r->n);
-                const bool first = batch.empty();
-                if (!first) {
+                if (r != head) {
                     if (int64_t(batch.size()) >= sv->opt.max_batch_sets) break;
-                    if (pts + r->n > sv->opt.max_batch_points) break;
                     if (sv->bytes_in_use + est + e > sv->opt.hbm_budget_bytes) break;
+                    if (r->n < lo || r->n > hi || pts + r->n > sv->opt.max_batch_points) {
+                        ++it;
+                        continue;
+                    }
                 }
-                sv->queue.pop_front();
+                it = sv->queue.erase(it);
                 r->t_admit = t;
                 batch.push_back(r);
                 pts += r->n;

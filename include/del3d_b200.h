@@ -258,12 +258,13 @@ void d3g_gen_lattice(int64_t n, double* xyz);
  * exactly what d3g_build returns for its points alone.
  *   - `slots` worker threads, each with its own CUDA stream: up to `slots`
  *     batches run on the device at once.
- *   - A free slot takes pending requests in arrival order while they fit: at
- *     most max_batch_sets requests and max_batch_points points per batch, and
- *     the estimated device memory of all in-flight batches within
- *     hbm_budget_bytes (a request larger than the budget runs alone once
- *     nothing else is in flight).  Requests arriving while batches run are
- *     admitted as soon as a slot and memory free up.
+ *   - A free slot takes the request at the head of the queue and, behind it,
+ *     requests of a similar size (within a factor 4) while they fit: at most
+ *     max_batch_sets requests and max_batch_points points per batch, and the
+ *     estimated device memory of all in-flight batches within hbm_budget_bytes
+ *     (a request larger than the budget runs alone once nothing else is in
+ *     flight).  Requests arriving while batches run are admitted as soon as a
+ *     slot and memory free up.
  *   - Points and tets stay on the device for the whole build; each request's
  *     cells are copied to a host buffer of its own.
  * Thread-safe: submit and wait may be called from any threads. */
