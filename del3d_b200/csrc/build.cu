@@ -2311,10 +2311,10 @@ void d3g_options_default(d3g_options* o) {
 
 void d3g_result_free(d3g_result* r) {
     if (!r) return;
-    free(r->cells);
-    free(r->all_cells);
-    free(r->incident_offsets);
-    free(r->incident);
+    host_result_free(r->cells);
+    host_result_free(r->all_cells);
+    host_result_free(r->incident_offsets);
+    host_result_free(r->incident);
     *r = d3g_result{};
 }
 
@@ -2349,17 +2349,17 @@ int d3g_build(const double* xyz, int64_t n, const d3g_options* opts, d3g_result*
         out->n_cells = R.n_cells;
         out->n_all = R.n_all;
         out->stats = R.stats;
-        out->cells = static_cast<int32_t*>(malloc(sizeof(int32_t) * 4 * size_t(R.n_cells > 0 ? R.n_cells : 1)));
+        out->cells = static_cast<int32_t*>(host_result_alloc(sizeof(int32_t) * 4 * size_t(R.n_cells > 0 ? R.n_cells : 1)));
         if (R.n_cells > 0)
             cudaMemcpyAsync(out->cells, R.cells.p, sizeof(int4) * R.n_cells, cudaMemcpyDeviceToHost, s);
         if (o.want_all_cells) {
-            out->all_cells = static_cast<int32_t*>(malloc(sizeof(int32_t) * 4 * size_t(R.n_all > 0 ? R.n_all : 1)));
+            out->all_cells = static_cast<int32_t*>(host_result_alloc(sizeof(int32_t) * 4 * size_t(R.n_all > 0 ? R.n_all : 1)));
             if (R.n_all > 0)
                 cudaMemcpyAsync(out->all_cells, R.all.p, sizeof(int4) * R.n_all, cudaMemcpyDeviceToHost, s);
         }
         if (o.want_incident) {
-            out->incident_offsets = static_cast<int64_t*>(malloc(sizeof(int64_t) * (size_t(n) + 1)));
-            out->incident = static_cast<int32_t*>(malloc(sizeof(int32_t) * size_t(R.n_inc > 0 ? R.n_inc : 1)));
+            out->incident_offsets = static_cast<int64_t*>(host_result_alloc(sizeof(int64_t) * (size_t(n) + 1)));
+            out->incident = static_cast<int32_t*>(host_result_alloc(sizeof(int32_t) * size_t(R.n_inc > 0 ? R.n_inc : 1)));
             cudaMemcpyAsync(out->incident_offsets, R.inc_off.p, sizeof(int64_t) * (n + 1),
                             cudaMemcpyDeviceToHost, s);
             if (R.n_inc > 0)
@@ -2416,9 +2416,9 @@ extern "C" {
 
 void d3g_batch_result_free(d3g_batch_result* r) {
     if (!r) return;
-    free(r->cell_offsets);
-    free(r->cells);
-    free(r->n_vertices);
+    host_result_free(r->cell_offsets);
+    host_result_free(r->cells);
+    host_result_free(r->n_vertices);
     *r = d3g_batch_result{};
 }
 
@@ -2449,9 +2449,9 @@ int d3g_build_batch(const double* xyz, const int64_t* set_offsets, int32_t n_set
     if (st == D3G_OK) {
         out->n_sets = n_sets;
         out->stats = R.stats;
-        out->cell_offsets = static_cast<int64_t*>(malloc(sizeof(int64_t) * (size_t(n_sets) + 1)));
-        out->n_vertices = static_cast<int64_t*>(malloc(sizeof(int64_t) * size_t(n_sets)));
-        out->cells = static_cast<int32_t*>(malloc(sizeof(int32_t) * 4 * size_t(R.n_cells > 0 ? R.n_cells : 1)));
+        out->cell_offsets = static_cast<int64_t*>(host_result_alloc(sizeof(int64_t) * (size_t(n_sets) + 1)));
+        out->n_vertices = static_cast<int64_t*>(host_result_alloc(sizeof(int64_t) * size_t(n_sets)));
+        out->cells = static_cast<int32_t*>(host_result_alloc(sizeof(int32_t) * 4 * size_t(R.n_cells > 0 ? R.n_cells : 1)));
         for (int i = 0; i <= n_sets; ++i) out->cell_offsets[i] = R.cell_off[size_t(i)];
         for (int i = 0; i < n_sets; ++i) out->n_vertices[i] = R.set_nv[size_t(i)];
         if (R.n_cells > 0)

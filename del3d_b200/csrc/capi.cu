@@ -3,7 +3,9 @@
 #include "common.cuh"
 
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <vector>
 #include <string>
 #include <vector>
 
@@ -68,6 +70,89 @@ int prepare_device() {
     return D3G_OK;
 }
 
+namespace {
+
+struct PinnedCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> free_blocks;     // size -> block, not in use
+    std::map<void*, size_t> pinned;               // every pinned block -> size
+    size_t cached_bytes = 0;                      // bytes in free_blocks
+};
+
+PinnedCache& pinned_cache() {
+    static PinnedCache* c = new PinnedCache();    // lives until exit (blocks freed by trim)
+    return *c;
+}
+
+// Blocks kept for reuse, at most this many bytes in all.
+constexpr size_t kPinnedCacheBytes = size_t(16) << 30;
+
+}  // namespace
+
+void* host_result_alloc(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    PinnedCache& c = pinned_cache();
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        // Smallest cached block that fits, if it is not more than twice the need.
+        auto it = c.free_blocks.lower_bound(bytes);
+        if (it != c.free_blocks.end() && it->first <= 2 * bytes) {
+            void* p = it->second;
+            c.cached_bytes -= it->first;
+            c.free_blocks.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) == cudaSuccess && p) {
+        std::lock_guard<std::mutex> lock(c.mu);
+        c.pinned[p] = bytes;
+        return p;
+    }
+    cudaGetLastError();
+    return malloc(bytes);
+}
+
+void host_result_free(void* p) {
+    if (!p) return;
+    PinnedCache& c = pinned_cache();
+    std::vector<void*> evict;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.pinned.find(p);
+        if (it == c.pinned.end()) {
+            free(p);
+            return;
+        }
+        c.free_blocks.emplace(it->second, p);
+        c.cached_bytes += it->second;
+        // Over the cap: drop the smallest cached blocks first.
+        while (c.cached_bytes > kPinnedCacheBytes && !c.free_blocks.empty()) {
+            auto f = c.free_blocks.begin();
+            c.cached_bytes -= f->first;
+            c.pinned.erase(f->second);
+            evict.push_back(f->second);
+            c.free_blocks.erase(f);
+        }
+    }
+    for (void* q : evict) cudaFreeHost(q);
+}
+
+void host_result_trim() {
+    PinnedCache& c = pinned_cache();
+    std::vector<void*> evict;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        for (auto& kv : c.free_blocks) {
+            c.pinned.erase(kv.second);
+            evict.push_back(kv.second);
+        }
+        c.free_blocks.clear();
+        c.cached_bytes = 0;
+    }
+    for (void* q : evict) cudaFreeHost(q);
+}
+
 }  // namespace d3g
 
 using namespace d3g;
@@ -95,6 +180,7 @@ const char* d3g_status_string(int status) {
 const char* d3g_last_error(void) { return g_last_error.c_str(); }
 
 int d3g_release_cached_memory(void) {
+    host_result_trim();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return D3G_ERR_NO_DEVICE;
     cudaMemPool_t pool;

@@ -73,6 +73,16 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = int64_t(kNumSMs) * 
     return unsigned(g);
 }
 
+/// Host memory for result arrays, from a cache of pinned (page-locked) blocks:
+/// device-to-host copies into it run at full PCIe rate, and a block handed back
+/// by host_result_free is reused by later results instead of being pinned again.
+/// Falls back to malloc if pinning fails.  host_result_free accepts any pointer
+/// host_result_alloc returned (and null).
+void* host_result_alloc(size_t bytes);
+void host_result_free(void* p);
+/// Unpins and frees the cached blocks not in use.
+void host_result_trim();
+
 /// Ensures a CUDA device is present and current, and prepares it.
 int ensure_device();
 /// Once per device: keeps freed stream-ordered allocations cached in the pool.

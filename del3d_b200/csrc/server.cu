@@ -132,7 +132,7 @@ int run_batch(const std::vector<Request*>& batch, cudaStream_t stream) {
             const int64_t a = R.cell_off[size_t(i)], b = R.cell_off[size_t(i) + 1];
             r->n_cells = b - a;
             r->n_vertices = R.set_nv[size_t(i)];
-            r->cells = static_cast<int32_t*>(std::malloc(sizeof(int4) * size_t(std::max<int64_t>(b - a, 1))));
+            r->cells = static_cast<int32_t*>(host_result_alloc(sizeof(int4) * size_t(std::max<int64_t>(b - a, 1))));
             if (!r->cells) {
                 set_error("d3g_server: host allocation failed");
                 st = D3G_ERR_OOM;
@@ -158,7 +158,7 @@ int run_batch(const std::vector<Request*>& batch, cudaStream_t stream) {
     for (Request* r : batch) {
         r->batch_sets = k;
         if (st != D3G_OK) {
-            std::free(r->cells);
+            host_result_free(r->cells);
             r->cells = nullptr;
             r->n_cells = r->n_vertices = 0;
             copy_error(r, st);
@@ -356,7 +356,7 @@ int d3g_server_wait(d3g_server* sv, int64_t ticket, double timeout_s, d3g_reques
 
 void d3g_request_result_free(d3g_request_result* r) {
     if (!r) return;
-    std::free(r->cells);
+    host_result_free(r->cells);
     r->cells = nullptr;
     r->n_cells = 0;
 }
@@ -386,7 +386,7 @@ int d3g_server_destroy(d3g_server* sv) {
     sv->cv_work.notify_all();
     for (std::thread& t : sv->workers) t.join();
     for (auto& kv : sv->requests) {
-        std::free(kv.second->cells);
+        host_result_free(kv.second->cells);
         delete kv.second;
     }
     delete sv;

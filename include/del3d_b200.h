@@ -54,8 +54,9 @@ const char* d3g_status_string(int status);
 const char* d3g_last_error(void);
 
 /* The library keeps device memory it frees cached in the current device's
- * stream-ordered pool (builds allocate gigabytes per call).  This returns the
- * cached memory to the driver; it synchronises the device. */
+ * stream-ordered pool (builds allocate gigabytes per call), and host result
+ * arrays in a cache of pinned blocks (freed results' blocks serve later ones,
+ * up to 16 GiB).  This returns both to the driver; it synchronises the device. */
 int d3g_release_cached_memory(void);
 
 /* ---- predicates ------------------------------------------------------------

@@ -81,3 +81,21 @@ def test_non_finite_rejected(cuda):
     pts[17, 1] = np.nan
     with pytest.raises(d3.Del3dError):
         d3.Delaunay().build(pts)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "clusters", "lattice", "sphere"])
+def test_schedules_and_lane_counts_agree(cuda, dist):
+    """The tet set does not depend on the insertion order, so the asynchronous
+    lock-based schedule, the lockstep rounds and every lane count must give the
+    same canonical cells, bit for bit, on every seed."""
+    import torch
+
+    for seed in range(3):
+        pts = d3.gen_set(dist, 40000 + 7919 * seed, 100 + seed)
+        x = torch.from_numpy(pts).to(cuda)
+        base, nv = d3.build_device(x, schedule=0)
+        base = base.clone()
+        for kw in ({"schedule": 1}, {"schedule": 1, "lanes": 8}, {"schedule": 1, "lanes": 4},
+                   {"schedule": 0, "chunk": -12, "alpha_small": 12}):
+            other, nv2 = d3.build_device(x, **kw)
+            assert nv2 == nv and torch.equal(other, base), (dist, seed, kw)
