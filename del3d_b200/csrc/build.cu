@@ -631,6 +631,7 @@ struct AsyncCtx {
     int* leftover;                  // points left for the rounds
     int* n_leftover;
     int64_t stride;                 // chunk q of the queue is chunk (q * stride) % W.n
+    unsigned long long* ekey;       // per warp slot: 3 edge keys per boundary facet (re-star)
     unsigned long long* stats;      // [0] lock conflicts, [1] walk restarts, [2] invalid seeds,
                                     // [3] regions too big, [4] points left, [5] first points left
 };
@@ -690,35 +691,6 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
         tv = nv;
     }
     return -1;
-}
-
-/// Neighbour across facet j of the new tet built on facet i of locked region
-/// tet c (see restar_neighbour); region membership is read from the locks.
-__device__ int restar_neighbour_locked(const Tables& T, const int* lock, int region, int c, const int4& cv,
-                                       int i, int j) {
-    int a = -1, b = -1;
-    for (int m = 0; m < 4; ++m)
-        if (m != i && m != j) {
-            if (a < 0) a = m;
-            else b = m;
-        }
-    const int va = at(cv, a), vb = at(cv, b);
-    int cur = c, f = j, steps = 0;
-    for (;;) {
-        const int enc = at(ld4(T.tn + cur), f);
-        const int nb = enc >> 2;
-        if (__ldcg(lock + nb) != region) {   // (cur, f) is a boundary facet
-            const int4 tc = ld4(T.tv + cur);
-            const int wpos = 6 - f - pos_of(tc, va) - pos_of(tc, vb);
-            if (wpos < 0 || wpos > 3 || wpos == f) return -1;
-            return __ldcg(T.fnew + cur * 4 + f) * 4 + wpos;
-        }
-        const int4 tb = ld4(T.tv + nb);
-        const int g = enc & 3;
-        f = 6 - g - pos_of(tb, va) - pos_of(tb, vb);
-        cur = nb;
-        if (f < 0 || f > 3 || f == g || ++steps > kRotateLimit) return -1;
-    }
 }
 
 enum : int { AI_DONE = 0, AI_RETRY = 1, AI_LEAVE = 2 };
@@ -852,21 +824,62 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         }
     }
     if (ok) {
-        for (int k = lane; k < F; k += 32) T.fnew[fac[k]] = k < C ? cav[k] : base + (k - C);
-        __syncwarp();
-        bool bad = false;
-        for (int k = lane; k < F && !bad; k += 32) {
+        // New tet k (on boundary facet (c, i), vertex i of c replaced by v) keeps
+        // c's outside neighbour across facet i.  Its facet j != i is v plus the
+        // edge of c's vertices at the other two positions; that edge lies on
+        // exactly one other boundary facet k2, where it is the edge of some
+        // facet j2 of new tet k2: the two new tets meet there, k2 facing back
+        // through j2.  Matching edge keys gives the same adjacency as turning
+        // round the edge inside the region (reference src/tds.h:160-221)
+        // without reading the mesh again.  Up to 32 facets the keys travel by
+        // warp shuffles, beyond that through the warp's key scratch.
+        unsigned long long* keys = A.ekey + int64_t(slot) * 3 * W.fac_cap;
+        for (int k = lane; k < F; k += 32) {
             const int c = fac[k] >> 2, i = fac[k] & 3;
             const int4 cv = ld4(T.tv + c);
-            int4 nv = cv, nn = ld4(T.tn + c);
+            int4 nv = cv;
             set_at(nv, i, v);
-            for (int j = 0; j < 4 && !bad; ++j) {
-                if (j == i) continue;
-                const int e = restar_neighbour_locked(T, A.lock, region, c, cv, i, j);
-                if (e < 0) bad = true;
-                else set_at(nn, j, e);
-            }
             sv[k] = nv;
+            sn[k] = ld4(T.tn + c);
+            int m = 0;
+            for (int j = 0; j < 4; ++j) {
+                if (j == i) continue;
+                int va = -2, vb = -2;
+                for (int q = 0; q < 4; ++q)
+                    if (q != i && q != j) {
+                        if (va == -2) va = at(cv, q);
+                        else vb = at(cv, q);
+                    }
+                const unsigned ua = unsigned(va + 1), ub = unsigned(vb + 1);
+                keys[3 * k + m] = ua < ub ? ((unsigned long long)ua << 32) | ub
+                                          : ((unsigned long long)ub << 32) | ua;
+                ++m;
+            }
+        }
+        __syncwarp();
+        bool bad = false;
+        for (int k = lane; k < F; k += 32) {
+            const int i = fac[k] & 3;
+            int4 nn = sn[k];
+            int m = 0;
+            for (int j = 0; j < 4; ++j) {
+                if (j == i) continue;
+                const unsigned long long key = keys[3 * k + m];
+                int found = -1, count = 0;
+                for (int q = 0; q < 3 * F; ++q)
+                    if (keys[q] == key && q / 3 != k) {
+                        found = q;
+                        ++count;
+                    }
+                if (count != 1) {
+                    bad = true;
+                } else {
+                    const int k2 = found / 3, m2 = found - 3 * k2, i2 = fac[k2] & 3;
+                    const int j2 = m2 + (m2 >= i2 ? 1 : 0);
+                    set_at(nn, j, (k2 < C ? cav[k2] : base + (k2 - C)) * 4 + j2);
+                }
+                ++m;
+            }
             sn[k] = nn;
         }
         if (__any_sync(kFull, bad)) {
@@ -1901,8 +1914,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     const bool use_async = opt.schedule != 1 && !grow;
     constexpr int kAsyncWarps = kNumSMs * 32;   // resident at 64 registers a thread
     DevBuf<int> alock, anext, aleft, anleft;
-    DevBuf<unsigned long long> astats;
+    DevBuf<unsigned long long> astats, aekey;
     if (use_async) {
+        D3G_TRY(aekey.alloc(size_t(std::min(maxw, kAsyncWarps)) * 3 * size_t(W.fac_cap), s));
         D3G_TRY(alock.alloc(size_t(T.cap), s));
         D3G_TRY(anext.alloc(1, s));
         D3G_TRY(aleft.alloc(size_t(nv), s));
@@ -2123,7 +2137,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             while (std::gcd(stride, int64_t(W.n)) != 1) ++stride;
             D3G_CUDA(cudaMemsetAsync(anext.p, 0, sizeof(int), s));
             D3G_CUDA(cudaMemsetAsync(anleft.p, 0, sizeof(int), s));
-            AsyncCtx A{alock.p, anext.p, aleft.p, anleft.p, stride, astats.p};
+            AsyncCtx A{alock.p, anext.p, aleft.p, anleft.p, stride, aekey.p, astats.p};
             const int warps = std::min(W.n, kAsyncWarps);
             unsigned long long won0 = 0;
             D3G_CUDA(cudaMemcpyAsync(&won0, totals.p, sizeof won0, cudaMemcpyDeviceToHost, s));
