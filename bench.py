@@ -33,6 +33,10 @@ One JSON line (rank 0):
               the same four distributions: points/s, requests/s and p50/p99
               latency per rate.
 
+Before the warm-up (not timed), d3g_autotune_device times the candidate speed
+settings (schedule, worker density, lanes) on every 8th set and makes the fastest
+the device default; the line reports the choice under "tuning".
+
 `--impl reference` times the reference's own CPU build on the same sample
 (rank 0 only; all host threads, one set per thread).
 """
@@ -87,6 +91,7 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="warm-up and timed steps only (no other legs): the command profiled by ncu")
     return ap.parse_args()
@@ -432,10 +437,23 @@ def run_ours(args):
     stream = torch.cuda.Stream(device=dev)
     handle = stream.cuda_stream
 
+    chunk = args.chunk or None          # None: the device default (tuned below)
+    tuning = None
+    if not args.no_autotune and not args.profile_run:
+        # Setup, not timed: time the candidate speed settings on a 1-in-8 sample
+        # of the sets and make the fastest this device's default.
+        sample = sets[::8]
+        soff = np.zeros(len(sample) + 1, dtype=np.int64)
+        soff[1:] = np.cumsum([a.shape[0] for a in sample])
+        xs = torch.from_numpy(np.concatenate(sample)).to(dev)
+        tuning = d3.autotune(xs, soff, stream=handle)
+        tuning["sample"] = f"every 8th set ({len(sample)} sets, {int(soff[-1])} points)"
+        del xs
+
     def step(stats=None, timing=False):
         if timing:
-            return _timed_batch(d3, x, offs, out, handle, args.chunk, stats)
-        return d3.build_batch_device(x, offs, out=out, stream=handle, chunk=args.chunk, stats=stats)
+            return _timed_batch(d3, x, offs, out, handle, chunk, stats)
+        return d3.build_batch_device(x, offs, out=out, stream=handle, chunk=chunk, stats=stats)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -487,7 +505,8 @@ def run_ours(args):
     lib = d3.library()
     opts = d3._Options()
     lib.d3g_options_default(ctypes.byref(opts))
-    opts.chunk = int(args.chunk)
+    if args.chunk:
+        opts.chunk = int(args.chunk)
 
     def e2e_call():
         res = d3._BatchResult()
@@ -581,7 +600,7 @@ def run_ours(args):
             "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
             "clocks": clk,
             "build_stats": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in stats.items()},
-            "cells": ncells, "generate_s": round(t_gen, 2),
+            "cells": ncells, "generate_s": round(t_gen, 2), "tuning": tuning,
         }
     if dist:
         dist.barrier()
@@ -610,7 +629,8 @@ def _timed_batch(d3, x, offs, out, handle, chunk, stats):
     nv = np.zeros(nsets, dtype=np.int64)
     opts = d3._Options()
     lib.d3g_options_default(ctypes.byref(opts))
-    opts.chunk = int(chunk)
+    if chunk:
+        opts.chunk = int(chunk)
     opts.timing = 1
     st = d3.BuildStats()
     d3._check(lib.d3g_build_batch_device(x.data_ptr(), offs.ctypes.data, nsets, ctypes.byref(opts),

@@ -111,6 +111,14 @@ class _ServerStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [("schedule", _I32), ("chunk", _I32), ("alpha_small", _I32), ("lanes", _I32),
+                ("ms", ctypes.c_double), ("candidates", _I32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class _PredStats(ctypes.Structure):
     _fields_ = [("n_queries", _I64), ("n_exact", _I64)]
 
@@ -173,6 +181,12 @@ def library() -> ctypes.CDLL:
     lib.d3g_server_destroy.restype = _INT
     lib.d3g_microbench_fp64.argtypes = [_I64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _P]
     lib.d3g_microbench_fp64.restype = _INT
+    lib.d3g_autotune_device.argtypes = [_P, _P, _I32, _P, ctypes.POINTER(_Tuning)]
+    lib.d3g_autotune_device.restype = _INT
+    lib.d3g_get_tuning.argtypes = [ctypes.POINTER(_Tuning)]
+    lib.d3g_get_tuning.restype = _INT
+    lib.d3g_reset_tuning.argtypes = []
+    lib.d3g_reset_tuning.restype = _INT
     lib.d3g_pool_usage.argtypes = [ctypes.POINTER(_I64), ctypes.POINTER(_I64), _INT]
     lib.d3g_pool_usage.restype = _INT
     lib.d3g_gen_uniform.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, _P]
@@ -376,7 +390,8 @@ class Delaunay:
         pts = _points(points)
         opts = _Options()
         lib.d3g_options_default(ctypes.byref(opts))
-        opts.chunk = int(chunk)
+        if chunk:
+            opts.chunk = int(chunk)
         opts.want_all_cells = int(all_cells)
         opts.want_incident = int(incident)
         res = _Result()
@@ -423,9 +438,17 @@ class Delaunay:
         return self._n_vertices
 
 
-def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: bool = False,
-                 stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0, lanes: int = 0,
-                 schedule: int = 0):
+def _apply(opts, **kw):
+    """Sets the options given (not None); the rest keep d3g_options_default's
+    values (which an autotuning run may have chosen)."""
+    for name, value in kw.items():
+        if value is not None:
+            setattr(opts, name, int(value))
+
+
+def build_device(points_dev, out=None, stream: int = 0, chunk: Optional[int] = None, timing: bool = False,
+                 stats: Optional[dict] = None, alpha_small: Optional[int] = None, split: Optional[int] = None,
+                 lanes: Optional[int] = None, schedule: Optional[int] = None):
     """Builds from a device-resident torch tensor (n, 3) float64 on `stream`
     (a raw cudaStream_t handle; 0 = default) and returns the canonical finite
     cells as a device int32 tensor view (n_cells, 4) and the vertex count.
@@ -441,12 +464,8 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: int = 0, timing: 
     nc, nv = _I64(0), _I64(0)
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
-    opts.chunk = int(chunk)
-    opts.timing = int(timing)
-    opts.alpha_small = int(alpha_small)
-    opts.split = int(split)
-    opts.lanes = int(lanes)
-    opts.schedule = int(schedule)
+    _apply(opts, chunk=chunk, timing=int(timing), alpha_small=alpha_small, split=split, lanes=lanes,
+           schedule=schedule)
     st = BuildStats()
     _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), out.shape[0],
                                 ctypes.byref(nc), ctypes.byref(nv), _P(stream), ctypes.byref(st)),
@@ -469,7 +488,8 @@ def build_batch(sets, chunk: int = 0, stats: Optional[dict] = None):
     xyz = np.ascontiguousarray(np.concatenate(arrays) if offs[-1] else np.zeros((1, 3)))
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
-    opts.chunk = int(chunk)
+    if chunk:
+        opts.chunk = int(chunk)
     res = _BatchResult()
     _check(lib.d3g_build_batch(_ptr(xyz), _ptr(offs), len(arrays), ctypes.byref(opts), ctypes.byref(res)),
            "build_batch")
@@ -487,9 +507,10 @@ def build_batch(sets, chunk: int = 0, stats: Optional[dict] = None):
     return [cells[co[i]:co[i + 1]] for i in range(len(arrays))], [int(v) for v in nv]
 
 
-def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk: int = 0,
-                       stats: Optional[dict] = None, alpha_small: int = 24, split: int = 0,
-                       lanes: int = 0, schedule: int = 0):
+def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk: Optional[int] = None,
+                       stats: Optional[dict] = None, alpha_small: Optional[int] = None,
+                       split: Optional[int] = None, lanes: Optional[int] = None,
+                       schedule: Optional[int] = None):
     """Device-resident form of build_batch: `points_dev` (n, 3) float64 CUDA
     tensor holding the sets back to back, `set_offsets` (n_sets + 1) host
     int64.  Returns the device cells tensor (all sets), the cell offsets per
@@ -506,11 +527,7 @@ def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk
     nv = np.zeros(nsets, dtype=np.int64)
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
-    opts.chunk = int(chunk)
-    opts.alpha_small = int(alpha_small)
-    opts.split = int(split)
-    opts.lanes = int(lanes)
-    opts.schedule = int(schedule)
+    _apply(opts, chunk=chunk, alpha_small=alpha_small, split=split, lanes=lanes, schedule=schedule)
     st = BuildStats()
     _check(lib.d3g_build_batch_device(x.data_ptr(), _ptr(offs), nsets, ctypes.byref(opts), out.data_ptr(),
                                       out.shape[0], _ptr(co), _ptr(nv), _P(stream), ctypes.byref(st)),
@@ -626,6 +643,30 @@ def pool_usage(reset_high: bool = False):
     u, h = _I64(0), _I64(0)
     _check(library().d3g_pool_usage(ctypes.byref(u), ctypes.byref(h), int(reset_high)), "pool_usage")
     return u.value, h.value
+
+
+# ---- autotuning ---------------------------------------------------------------------
+
+
+def autotune(points_dev, set_offsets, stream: int = 0) -> dict:
+    """Times builds of the sets `set_offsets` of the device tensor `points_dev`
+    under the candidate speed settings and makes the fastest this device's
+    default (d3g_autotune_device).  Returns the chosen setting."""
+    offs = np.ascontiguousarray(set_offsets, dtype=np.int64)
+    t = _Tuning()
+    _check(library().d3g_autotune_device(points_dev.contiguous().data_ptr(), _ptr(offs), offs.shape[0] - 1,
+                                         _P(stream), ctypes.byref(t)), "autotune")
+    return t.as_dict()
+
+
+def get_tuning() -> dict:
+    t = _Tuning()
+    _check(library().d3g_get_tuning(ctypes.byref(t)), "get_tuning")
+    return t.as_dict()
+
+
+def reset_tuning() -> None:
+    _check(library().d3g_reset_tuning(), "reset_tuning")
 
 
 # ---- synthetic inputs -------------------------------------------------------------

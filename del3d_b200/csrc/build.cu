@@ -35,6 +35,7 @@
 #include "device_util.cuh"
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
 #include <cmath>
 #include <cstdio>
@@ -2308,6 +2309,31 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
 
 using namespace d3g;
 
+namespace d3g {
+namespace {
+
+// The settings d3g_autotune_device chose, per device (d3g_options_default
+// hands them out).
+constexpr int kMaxTunedDevices = 64;
+std::mutex g_tuning_mu;
+d3g_tuning g_tuning[kMaxTunedDevices];
+bool g_tuned[kMaxTunedDevices] = {};
+
+bool current_tuning(d3g_tuning* out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxTunedDevices) {
+        cudaGetLastError();
+        return false;
+    }
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
+    if (!g_tuned[dev]) return false;
+    *out = g_tuning[dev];
+    return true;
+}
+
+}  // namespace
+}  // namespace d3g
+
 extern "C" {
 
 void d3g_options_default(d3g_options* o) {
@@ -2321,6 +2347,100 @@ void d3g_options_default(d3g_options* o) {
     o->lanes = 0;
     o->schedule = 0;
     o->split = 0;
+    d3g_tuning t;
+    if (current_tuning(&t)) {
+        o->schedule = t.schedule;
+        o->chunk = t.chunk;
+        o->alpha_small = t.alpha_small;
+        o->lanes = t.lanes;
+    }
+}
+
+int d3g_get_tuning(d3g_tuning* out) {
+    if (!out) return D3G_ERR_INVALID_ARGUMENT;
+    if (!current_tuning(out)) {
+        d3g_options o;
+        d3g_options_default(&o);
+        *out = d3g_tuning{o.schedule, o.chunk, o.alpha_small, o.lanes, 0.0, 0};
+    }
+    return D3G_OK;
+}
+
+int d3g_reset_tuning(void) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxTunedDevices) {
+        cudaGetLastError();
+        return D3G_ERR_NO_DEVICE;
+    }
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
+    g_tuned[dev] = false;
+    return D3G_OK;
+}
+
+int d3g_autotune_device(const double* d_xyz, const int64_t* set_offsets, int32_t n_sets, void* stream,
+                        d3g_tuning* best) {
+    if (n_sets < 1 || !set_offsets || set_offsets[0] != 0 || set_offsets[n_sets] < 0 ||
+        (set_offsets[n_sets] > 0 && !d_xyz))
+        return D3G_ERR_INVALID_ARGUMENT;
+    D3G_TRY(ensure_device());
+    int dev = 0;
+    D3G_CUDA(cudaGetDevice(&dev));
+    if (dev >= kMaxTunedDevices) return D3G_ERR_NO_DEVICE;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // Candidates: the schedule, the worker density (one worker per `alpha`
+    // earlier points, denser below one wave: `alpha_small`) and, for the
+    // lockstep rounds, the lanes per worker.  Every setting gives the same
+    // cells; only the time differs.
+    struct Cand { int schedule, alpha, alpha_small, lanes; };
+    std::vector<Cand> cands;
+    for (int a : {24, 48, 96})
+        for (int as : {12, 24}) cands.push_back({0, a, as, 0});
+    for (int a : {24, 48})
+        for (int l : {32, 16}) cands.push_back({1, a, 24, l});
+    cudaEvent_t e0, e1;
+    D3G_CUDA(cudaEventCreate(&e0));
+    D3G_CUDA(cudaEventCreate(&e1));
+    d3g_tuning win{0, 0, 24, 0, 1e30, 0};
+    int st = D3G_OK;
+    for (const Cand& c : cands) {
+        d3g_options o;
+        d3g_options_default(&o);
+        o.want_all_cells = 0;
+        o.want_incident = 0;
+        o.schedule = c.schedule;
+        o.chunk = -c.alpha;
+        o.alpha_small = c.alpha_small;
+        o.lanes = c.lanes;
+        float best_ms = 1e30f;
+        for (int rep = 0; rep < 2 && st == D3G_OK; ++rep) {   // first run warms the pool
+            DeviceResult R;
+            cudaEventRecord(e0, s == nullptr ? cudaStreamLegacy : s);
+            st = build_on_stream(d_xyz, set_offsets, n_sets, o, s, R);
+            cudaEventRecord(e1, s == nullptr ? cudaStreamLegacy : s);
+            R.reset();
+            if (st != D3G_OK) break;
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                st = D3G_ERR_CUDA;
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) best_ms = ms;
+        }
+        if (st != D3G_OK) break;
+        win.candidates += 1;
+        if (best_ms < win.ms) win = d3g_tuning{c.schedule, -c.alpha, c.alpha_small, c.lanes, best_ms, win.candidates};
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != D3G_OK) return st;
+    {
+        std::lock_guard<std::mutex> lock(g_tuning_mu);
+        g_tuning[dev] = win;
+        g_tuned[dev] = true;
+    }
+    if (best) *best = win;
+    return D3G_OK;
 }
 
 void d3g_result_free(d3g_result* r) {

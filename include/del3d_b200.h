@@ -315,6 +315,25 @@ int d3g_server_destroy(d3g_server* s);
  * mark since the last reset (reset_high != 0 resets it). */
 int d3g_pool_usage(int64_t* used, int64_t* used_high, int reset_high);
 
+/* ---- autotuning -----------------------------------------------------------------
+ * Times builds of the given (device-resident) sets under candidate settings of
+ * the options that only change speed - schedule, worker density (chunk as
+ * -alpha, alpha_small) and lanes per worker - and makes the fastest the default
+ * that d3g_options_default returns on this device from then on.  Every setting
+ * gives the same cells.  Runs 2 builds per candidate (10 candidates); pass a
+ * sample of the workload.  No counterpart in the reference. */
+typedef struct d3g_tuning {
+    int32_t schedule, chunk, alpha_small, lanes;  /* the chosen option values        */
+    double ms;                                   /* its build time on the sample     */
+    int32_t candidates;                          /* settings timed                   */
+} d3g_tuning;
+int d3g_autotune_device(const double* d_xyz, const int64_t* set_offsets, int32_t n_sets, void* stream,
+                        d3g_tuning* best);
+/* The current device's tuned settings (the built-in defaults if never tuned). */
+int d3g_get_tuning(d3g_tuning* out);
+/* Forgets the current device's tuning. */
+int d3g_reset_tuning(void);
+
 /* ---- measurement aid ------------------------------------------------------------
  * FP64 throughput of the current device with the filters' arithmetic: separate
  * DADD/DMUL operations per second (the filters are built without contraction)
