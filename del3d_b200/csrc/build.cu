@@ -168,6 +168,16 @@ __device__ __forceinline__ int orient_replaced(const Pt* q, int i, const Pt& p, 
     return orient3d_x(A, B, C, D, ex, st);
 }
 
+/// coplanar_in_circle for the hull case of the conflict test (rare: the point
+/// lies in the plane of a hull facet), out of line so that its code stays out
+/// of the hot path's instruction stream.
+__device__ __noinline__ int hull_in_circle(double ax, double ay, double az, double bx, double by, double bz,
+                                           double dx, double dy, double dz, double px, double py, double pz,
+                                           int ia, int ib, int id_, int ip, uint32_t* st) {
+    const int64_t id[4] = {ia, ib, id_, ip};
+    return coplanar_in_circle(Pt{ax, ay, az}, Pt{bx, by, bz}, Pt{dx, dy, dz}, Pt{px, py, pz}, id, st);
+}
+
 /// The reference's conflict test, src/triangulation.cpp:588-602.  `ex`: the
 /// point set's coordinates span few enough bits that the orient3d and in_sphere
 /// filters compute their determinants exactly.
@@ -184,8 +194,7 @@ __device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __
         const Pt a = vpt(vx, va), b = vpt(vx, vb), d = vpt(vx, vd);
         const int s = orient3d_x(a, b, d, p, ex, st);
         if (s != 0) return s > 0;
-        const int64_t id[4] = {va, vb, vd, pid};
-        return coplanar_in_circle(a, b, d, p, id, st) > 0;
+        return hull_in_circle(a.x, a.y, a.z, b.x, b.y, b.z, d.x, d.y, d.z, p.x, p.y, p.z, va, vb, vd, pid, st) > 0;
     }
     const Pt a = vpt(vx, t.x), b = vpt(vx, t.y), c = vpt(vx, t.z), d = vpt(vx, t.w);
     const InSphereFilter f = in_sphere_filter(a, b, c, d, p);
@@ -195,6 +204,13 @@ __device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __
                                         t.x, t.y, t.z, t.w, pid, st) > 0;
     return in_sphere_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, p.x, p.y, p.z, t.x,
                                 t.y, t.z, t.w, pid, f.det, 1, st) > 0;
+}
+
+/// in_conflict out of line, for the once-per-insertion seed check (one inline
+/// copy, in the breadth-first growth, is enough for the hot path).
+__device__ __noinline__ bool in_conflict_seed(int4 t, double px, double py, double pz, int pid,
+                                              const double* __restrict__ vx, bool ex, uint32_t* st) {
+    return in_conflict(t, Pt{px, py, pz}, pid, vx, ex, st);
 }
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -718,7 +734,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         int seen = 0;
         if (!try_lock(A.lock, seed, region, &seen)) {
             res = 1;
-        } else if (!__ldcg(T.alive + seed) || !in_conflict(ld4(T.tv + seed), p, v, vx, ex, st)) {
+        } else if (!__ldcg(T.alive + seed) || !in_conflict_seed(ld4(T.tv + seed), p.x, p.y, p.z, v, vx, ex, st)) {
             unlock_if(A.lock, seed, region);
             res = 2;
         } else {
