@@ -639,10 +639,17 @@ def fp64_throughput(iters: int = 1 << 16, stream: int = 0):
 
 
 def pool_usage(reset_high: bool = False):
-    """(bytes in use, high-water mark) of the current device's stream-ordered pool."""
+    """(bytes in use, high-water mark) of the current device's stream-ordered
+    pool; blocks the library keeps cached for later builds count as in use."""
     u, h = _I64(0), _I64(0)
     _check(library().d3g_pool_usage(ctypes.byref(u), ctypes.byref(h), int(reset_high)), "pool_usage")
     return u.value, h.value
+
+
+def release_cached_memory() -> None:
+    """Returns the cached device blocks and the pool's reserve to the driver and
+    unpins the cached host result blocks (synchronises the device)."""
+    _check(library().d3g_release_cached_memory(), "release_cached_memory")
 
 
 # ---- autotuning ---------------------------------------------------------------------

@@ -1547,7 +1547,7 @@ int sort_cells(DevBuf<int4>& cells, DevBuf<unsigned long long>& khi, DevBuf<unsi
         D3G_TRY(sk2.alloc(size_t(n), s));
         k_gather_i32<<<grid_for(n, 256), 256, 0, s>>>(cset, idx.p, n, sk.p);
         D3G_TRY(sort_pairs(sk.p, sk2.p, idx.p, i2.p, n, 0, bits_for(uint64_t(nsets)), s));
-        std::swap(idx.p, i2.p);
+        idx.swap(i2);
     }
     k_gather_cells<<<grid_for(n, 256), 256, 0, s>>>(cells.p, idx.p, n, out.p);
     D3G_CUDA(cudaGetLastError());
@@ -1662,7 +1662,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                                                           ranks.p);
             D3G_TRY(sort_pairs(keys.p, keys2.p, ranks.p, sranks.p, n, 0,
                                key_axis == 3 ? bits_for(uint64_t(nsets)) : 64, s));
-            std::swap(ranks.p, sranks.p);
+            ranks.swap(sranks);
         }
         D3G_TRY(first.alloc(size_t(N), s));
         D3G_TRY(rep.alloc(size_t(N), s));

@@ -2,6 +2,7 @@
 // device entry points, synthetic input generators.
 #include "common.cuh"
 
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -153,6 +154,213 @@ void host_result_trim() {
     for (void* q : evict) cudaFreeHost(q);
 }
 
+namespace {
+
+struct IdleBlock {
+    void* p;
+    cudaStream_t s;     // stream of its last use
+    cudaEvent_t ev;     // recorded on s when the block was handed back
+    uint64_t age;       // hand-back order: the oldest is evicted first
+};
+
+struct DeviceBlockCache {
+    std::mutex mu;
+    std::multimap<size_t, IdleBlock> idle;   // size -> block not in use
+    std::vector<cudaEvent_t> events;         // spare events of this device
+    size_t idle_bytes = 0;
+    size_t limit = 0;                        // idle bytes kept: a quarter of the device memory
+    uint64_t clock = 0;
+};
+
+constexpr int kMaxDevices = 64;
+
+DeviceBlockCache& block_cache(int dev) {
+    static DeviceBlockCache* c = new DeviceBlockCache[kMaxDevices];   // lives until exit
+    return c[dev];
+}
+
+bool is_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return st != cudaStreamCaptureStatusNone;
+}
+
+cudaEvent_t take_event(DeviceBlockCache& c) {
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        if (!c.events.empty()) {
+            cudaEvent_t ev = c.events.back();
+            c.events.pop_back();
+            return ev;
+        }
+    }
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return ev;
+}
+
+void give_event(DeviceBlockCache& c, cudaEvent_t ev) {
+    std::lock_guard<std::mutex> lock(c.mu);
+    c.events.push_back(ev);
+}
+
+/// Returns idle blocks to the pool in the order of `s`, after their last use.
+void free_idle_on(DeviceBlockCache& c, std::vector<IdleBlock>& blocks, cudaStream_t s) {
+    for (IdleBlock& b : blocks) {
+        if (b.s != s && cudaStreamWaitEvent(s, b.ev, 0) != cudaSuccess) cudaGetLastError();
+        if (cudaFreeAsync(b.p, s) != cudaSuccess) cudaGetLastError();
+        give_event(c, b.ev);
+    }
+    blocks.clear();
+}
+
+}  // namespace
+
+cudaError_t device_block_alloc(void** p, size_t bytes, cudaStream_t s, size_t* cap, int* dev) {
+    *cap = 0;
+    *dev = -1;
+    int d = -1;
+    if (bytes >= kBlockCacheMin && cudaGetDevice(&d) != cudaSuccess) {
+        cudaGetLastError();
+        d = -1;
+    }
+    if (bytes < kBlockCacheMin || d < 0 || d >= kMaxDevices || is_capturing(s))
+        return cudaMallocAsync(p, bytes, s);
+    DeviceBlockCache& c = block_cache(d);
+    bool hit = false;
+    size_t size = 0;
+    IdleBlock b{};
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        if (c.limit == 0) {
+            size_t free_b = 0, total_b = 0;
+            if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) cudaGetLastError();
+            c.limit = std::max<size_t>(total_b / 4, size_t(1) << 30);
+        }
+        // The smallest idle block that fits, if it wastes at most a quarter.
+        auto it = c.idle.lower_bound(bytes);
+        if (it != c.idle.end() && it->first - bytes <= bytes / 4) {
+            hit = true;
+            size = it->first;
+            b = it->second;
+            c.idle_bytes -= size;
+            c.idle.erase(it);
+        }
+    }
+    if (hit) {
+        if (b.s == s || cudaStreamWaitEvent(s, b.ev, 0) == cudaSuccess) {
+            give_event(c, b.ev);
+            *p = b.p;
+            *cap = size;
+            *dev = d;
+            return cudaSuccess;
+        }
+        cudaGetLastError();
+        std::vector<IdleBlock> one{b};
+        free_idle_on(c, one, b.s);
+    }
+    cudaError_t e = cudaMallocAsync(p, bytes, s);
+    if (e == cudaErrorMemoryAllocation) {
+        // Idle blocks of other sizes go back to the pool, which may then fit the request.
+        cudaGetLastError();
+        std::vector<IdleBlock> all;
+        {
+            std::lock_guard<std::mutex> lock(c.mu);
+            for (auto& kv : c.idle) all.push_back(kv.second);
+            c.idle.clear();
+            c.idle_bytes = 0;
+        }
+        if (!all.empty()) {
+            free_idle_on(c, all, s);
+            e = cudaMallocAsync(p, bytes, s);
+        }
+    }
+    if (e == cudaSuccess) {
+        *cap = bytes;
+        *dev = d;
+    }
+    return e;
+}
+
+void device_block_free(void* p, size_t cap, cudaStream_t s, int dev) {
+    if (!p) return;
+    if (cap == 0 || dev < 0 || dev >= kMaxDevices || is_capturing(s)) {
+        cudaFreeAsync(p, s);
+        return;
+    }
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) cudaGetLastError();
+    if (cur != dev && cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeAsync(p, s);
+        return;
+    }
+    DeviceBlockCache& c = block_cache(dev);
+    cudaEvent_t ev = take_event(c);
+    if (!ev || cudaEventRecord(ev, s) != cudaSuccess) {
+        cudaGetLastError();
+        if (ev) give_event(c, ev);
+        if (cudaFreeAsync(p, s) != cudaSuccess) cudaGetLastError();
+    } else {
+        std::vector<IdleBlock> evict;
+        {
+            std::lock_guard<std::mutex> lock(c.mu);
+            c.idle.emplace(cap, IdleBlock{p, s, ev, ++c.clock});
+            c.idle_bytes += cap;
+            while (c.idle_bytes > c.limit && !c.idle.empty()) {
+                auto oldest = c.idle.begin();
+                for (auto it = c.idle.begin(); it != c.idle.end(); ++it)
+                    if (it->second.age < oldest->second.age) oldest = it;
+                c.idle_bytes -= oldest->first;
+                evict.push_back(oldest->second);
+                c.idle.erase(oldest);
+            }
+        }
+        free_idle_on(c, evict, s);
+    }
+    if (cur != dev && cur >= 0 && cudaSetDevice(cur) != cudaSuccess) cudaGetLastError();
+}
+
+int device_block_trim() {
+    int d = -1;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) {
+        cudaGetLastError();
+        return D3G_ERR_NO_DEVICE;
+    }
+    DeviceBlockCache& c = block_cache(d);
+    std::vector<IdleBlock> all;
+    std::vector<cudaEvent_t> events;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        for (auto& kv : c.idle) all.push_back(kv.second);
+        c.idle.clear();
+        c.idle_bytes = 0;
+        events.swap(c.events);
+    }
+    // The caller has synchronised the device: every idle block's last use is
+    // over, and the legacy stream orders the frees (the stream of a block's last
+    // use may be gone by now).
+    cudaError_t first = cudaSuccess;
+    auto note = [&](cudaError_t e) {
+        if (e != cudaSuccess && first == cudaSuccess) first = e;
+    };
+    for (IdleBlock& b : all) {
+        note(cudaFreeAsync(b.p, cudaStreamLegacy));
+        note(cudaEventDestroy(b.ev));
+    }
+    for (cudaEvent_t ev : events) note(cudaEventDestroy(ev));
+    if (first == cudaSuccess) return D3G_OK;
+    cudaGetLastError();
+    set_error(std::string("releasing cached device blocks: ") + cudaGetErrorString(first));
+    return D3G_ERR_CUDA;
+}
+
 }  // namespace d3g
 
 using namespace d3g;
@@ -185,6 +393,8 @@ int d3g_release_cached_memory(void) {
     if (cudaGetDevice(&dev) != cudaSuccess) return D3G_ERR_NO_DEVICE;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return D3G_ERR_CUDA;
+    if (cudaDeviceSynchronize() != cudaSuccess) return D3G_ERR_CUDA;
+    D3G_TRY(device_block_trim());
     if (cudaDeviceSynchronize() != cudaSuccess) return D3G_ERR_CUDA;
     return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? D3G_OK : D3G_ERR_CUDA;
 }

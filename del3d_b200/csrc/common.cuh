@@ -9,6 +9,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 
 namespace d3g {
 
@@ -35,12 +36,32 @@ int status_from_bits(uint32_t bits);
         if (s_ != D3G_OK) return s_;   \
     } while (0)
 
+/// Stream-ordered device memory.  Blocks of kBlockCacheMin bytes and more go
+/// through a per-device cache: a freed block waits there, with an event that
+/// marks the end of its last use, and serves a later request of about its size
+/// on any stream (which first waits for that event).  Repeated builds of one
+/// workload then make no large pool calls: a large cudaMallocAsync can hold the
+/// calling thread for hundreds of milliseconds even when the pool already
+/// reserves the memory, while the device sits idle.  Smaller blocks, and blocks
+/// of a stream under graph capture, go to the pool directly.
+constexpr size_t kBlockCacheMin = size_t(1) << 20;
+/// Allocates at least `bytes` on `s`; `*cap` receives the block's size when it
+/// belongs to the cache (0 otherwise) and `*dev` its device.
+cudaError_t device_block_alloc(void** p, size_t bytes, cudaStream_t s, size_t* cap, int* dev);
+/// Hands back a block from device_block_alloc after the work queued on `s`.
+void device_block_free(void* p, size_t cap, cudaStream_t s, int dev);
+/// Returns the current device's cached blocks not in use to the pool; the
+/// device must be synchronised.
+int device_block_trim();
+
 /// A stream-ordered device allocation, freed on the same stream.
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
     cudaStream_t s = nullptr;
+    size_t cap = 0;     // size of a cached block, 0 for a pool block
+    int dev = -1;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
@@ -50,7 +71,7 @@ struct DevBuf {
         s = stream;
         n = count;
         if (count == 0) return D3G_OK;
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), stream);
+        cudaError_t e = device_block_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), stream, &cap, &dev);
         if (e != cudaSuccess) {
             p = nullptr;
             n = 0;
@@ -60,9 +81,18 @@ struct DevBuf {
         return D3G_OK;
     }
     void release() {
-        if (p) cudaFreeAsync(p, s);
+        if (p) device_block_free(p, cap, s, dev);
         p = nullptr;
         n = 0;
+        cap = 0;
+    }
+    /// Exchanges the blocks of two buffers (ping-pong passes).
+    void swap(DevBuf& o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+        std::swap(s, o.s);
+        std::swap(cap, o.cap);
+        std::swap(dev, o.dev);
     }
 };
 

@@ -53,10 +53,13 @@ const char* d3g_status_string(int status);
 /* Detail of the last error on the calling thread ("" if none). */
 const char* d3g_last_error(void);
 
-/* The library keeps device memory it frees cached in the current device's
- * stream-ordered pool (builds allocate gigabytes per call), and host result
- * arrays in a cache of pinned blocks (freed results' blocks serve later ones,
- * up to 16 GiB).  This returns both to the driver; it synchronises the device. */
+/* The library keeps device memory it frees for later calls (builds allocate
+ * gigabytes per call): blocks of 1 MiB and more in its own cache, which hands a
+ * block to a later request of about its size on any stream (idle blocks up to a
+ * quarter of the device memory), the rest in the current device's stream-ordered
+ * pool.  Host result arrays come from a cache of pinned blocks (freed results'
+ * blocks serve later ones, up to 16 GiB).  This returns all of them to the
+ * driver; it synchronises the device. */
 int d3g_release_cached_memory(void);
 
 /* ---- predicates ------------------------------------------------------------
@@ -311,8 +314,9 @@ int d3g_server_get_stats(d3g_server* s, d3g_server_stats* out);
  * results not collected. */
 int d3g_server_destroy(d3g_server* s);
 
-/* The current device's stream-ordered pool: bytes in use and the high-water
- * mark since the last reset (reset_high != 0 resets it). */
+/* The current device's stream-ordered pool: bytes in use (the library's
+ * cached blocks included) and the high-water mark since the last reset
+ * (reset_high != 0 resets it). */
 int d3g_pool_usage(int64_t* used, int64_t* used_high, int reset_high);
 
 /* ---- autotuning -----------------------------------------------------------------
