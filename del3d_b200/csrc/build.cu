@@ -712,6 +712,23 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
 
 enum : int { AI_DONE = 0, AI_RETRY = 1, AI_LEAVE = 2 };
 
+/// Key of the edge (a, b), either order.
+__device__ __forceinline__ unsigned long long edge_key(int a, int b) {
+    const unsigned ua = unsigned(a + 1), ub = unsigned(b + 1);
+    return ua < ub ? ((unsigned long long)ua << 32) | ub : ((unsigned long long)ub << 32) | ua;
+}
+
+/// Edge keys of facets p0 < p1 < p2 (the positions other than i) of a tet with
+/// vertices c: facet j's edge joins the two positions other than i and j.
+__device__ __forceinline__ void facet_edge_keys(const int4 c, int i, unsigned long long& e0,
+                                                unsigned long long& e1, unsigned long long& e2) {
+    const int p0 = i == 0 ? 1 : 0, p1 = i <= 1 ? 2 : 1, p2 = i <= 2 ? 3 : 2;
+    const int a0 = at(c, p0), a1 = at(c, p1), a2 = at(c, p2);
+    e0 = edge_key(a1, a2);
+    e1 = edge_key(a0, a2);
+    e2 = edge_key(a0, a1);
+}
+
 /// One insertion of point v by the whole warp, starting the walk at tet t0.
 /// AI_DONE: inserted; AI_RETRY: a lock was taken by another warp (nothing
 /// changed, every lock given back); AI_LEAVE: leave it for the rounds.
@@ -848,8 +865,9 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         // facet j2 of new tet k2: the two new tets meet there, k2 facing back
         // through j2.  Matching edge keys gives the same adjacency as turning
         // round the edge inside the region (reference src/tds.h:160-221)
-        // without reading the mesh again.  Up to 32 facets the keys travel by
-        // warp shuffles, beyond that through the warp's key scratch.
+        // without reading the mesh again.  The keys go through the warp's key
+        // scratch, which stays in L1 (a shared-memory hash table per warp was
+        // slower: the shared memory it takes comes out of L1).
         unsigned long long* keys = A.ekey + int64_t(slot) * 3 * W.fac_cap;
         for (int k = lane; k < F; k += 32) {
             const int c = fac[k] >> 2, i = fac[k] & 3;
@@ -858,45 +876,43 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             set_at(nv, i, v);
             sv[k] = nv;
             sn[k] = ld4(T.tn + c);
-            int m = 0;
-            for (int j = 0; j < 4; ++j) {
-                if (j == i) continue;
-                int va = -2, vb = -2;
-                for (int q = 0; q < 4; ++q)
-                    if (q != i && q != j) {
-                        if (va == -2) va = at(cv, q);
-                        else vb = at(cv, q);
-                    }
-                const unsigned ua = unsigned(va + 1), ub = unsigned(vb + 1);
-                keys[3 * k + m] = ua < ub ? ((unsigned long long)ua << 32) | ub
-                                          : ((unsigned long long)ub << 32) | ua;
-                ++m;
-            }
+            facet_edge_keys(cv, i, keys[3 * k], keys[3 * k + 1], keys[3 * k + 2]);
         }
         __syncwarp();
         bool bad = false;
         for (int k = lane; k < F; k += 32) {
+            // One pass over the keys of every other facet finds the partners of
+            // all three edges (key m of facet k2 is its edge m: each edge key
+            // must occur on exactly one other facet).  The lanes walk the keys
+            // in step, so every load is a broadcast.
+            const unsigned long long e0 = keys[3 * k], e1 = keys[3 * k + 1], e2 = keys[3 * k + 2];
+            int f0 = -1, f1 = -1, f2 = -1, n0 = 0, n1 = 0, n2 = 0;
+            for (int o = 0; o < F; ++o) {
+                const bool other = o != k;
+#pragma unroll
+                for (int m2 = 0; m2 < 3; ++m2) {
+                    const unsigned long long key = keys[3 * o + m2];
+                    const int q = 3 * o + m2;
+                    if (other && key == e0) { f0 = q; ++n0; }
+                    if (other && key == e1) { f1 = q; ++n1; }
+                    if (other && key == e2) { f2 = q; ++n2; }
+                }
+            }
             const int i = fac[k] & 3;
             int4 nn = sn[k];
-            int m = 0;
-            for (int j = 0; j < 4; ++j) {
-                if (j == i) continue;
-                const unsigned long long key = keys[3 * k + m];
-                int found = -1, count = 0;
-                for (int q = 0; q < 3 * F; ++q)
-                    if (keys[q] == key && q / 3 != k) {
-                        found = q;
-                        ++count;
-                    }
+            // Facet j of new tet k (j != i, increasing) carries edge key m = 0, 1, 2.
+            auto link = [&](int j, int found, int count) {
                 if (count != 1) {
                     bad = true;
-                } else {
-                    const int k2 = found / 3, m2 = found - 3 * k2, i2 = fac[k2] & 3;
-                    const int j2 = m2 + (m2 >= i2 ? 1 : 0);
-                    set_at(nn, j, (k2 < C ? cav[k2] : base + (k2 - C)) * 4 + j2);
+                    return;
                 }
-                ++m;
-            }
+                const int k2 = found / 3, m2 = found - 3 * k2, i2 = fac[k2] & 3;
+                const int j2 = m2 + (m2 >= i2 ? 1 : 0);
+                set_at(nn, j, (k2 < C ? cav[k2] : base + (k2 - C)) * 4 + j2);
+            };
+            link(i == 0 ? 1 : 0, f0, n0);
+            link(i <= 1 ? 2 : 1, f1, n1);
+            link(i <= 2 ? 3 : 2, f2, n2);
             sn[k] = nn;
         }
         if (__any_sync(kFull, bad)) {
