@@ -47,3 +47,15 @@ def test_bad_arguments_rejected_without_device():
     # Null output / negative sizes are rejected before any device work.
     assert lib.d3g_build(None, -1, None, None) == 1
     assert lib.d3g_predicates(None, 0, None, -5, 0, None, None) == 1
+
+
+def test_memory_calls_without_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    # Releasing the caches and reading the pool need a device; both report it.
+    with pytest.raises(del3d_b200.Del3dError):
+        del3d_b200.release_cached_memory()
+    with pytest.raises(del3d_b200.Del3dError):
+        del3d_b200.pool_usage()
