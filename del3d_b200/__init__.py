@@ -10,9 +10,11 @@ It mirrors the reference's public interface (``include/del3d/delaunay.h``,
   :func:`orient2d`, :func:`coplanar_orientation`, :func:`coplanar_in_circle`,
   :func:`coplanar_in_circle_unperturbed`, :func:`collinear` - batched over index
   tuples into one point table;
-* :func:`spatial_sort` - the reference insertion order, bit for bit.
+* :func:`spatial_sort` - the reference insertion order, bit for bit;
+* :func:`load_mesh`, :func:`weld`, :func:`drop_non_finite`, :func:`read_xyz`,
+  :func:`load_point_sets` - the reference viewer's input readers, on the host.
 
-Everything runs on the GPU; there is no CPU fallback.  Importing works without a
+Everything but the input readers runs on the GPU; there is no CPU fallback.  Importing works without a
 GPU (the library loads), but every call then fails with :class:`Del3dError`.
 
 One documented difference: ``finite_cells()`` comes back in a canonical order
@@ -33,6 +35,8 @@ __all__ = [
     "orient2d", "coplanar_orientation", "coplanar_in_circle", "coplanar_in_circle_unperturbed",
     "collinear", "spatial_sort", "library", "LIB_PATH", "predicate_stats", "circumcenters",
     "circumcenter", "circumcenter_lazy", "Server", "Request", "pool_usage",
+    "release_cached_memory", "load_mesh", "read_xyz", "weld", "drop_non_finite",
+    "supported_formats", "load_point_sets",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -123,6 +127,16 @@ class _PredStats(ctypes.Structure):
     _fields_ = [("n_queries", _I64), ("n_exact", _I64)]
 
 
+class _Mesh(ctypes.Structure):
+    _fields_ = [("vertices", ctypes.POINTER(ctypes.c_double)), ("faces", ctypes.POINTER(_I32)),
+                ("n_vertices", _I64), ("n_faces", _I64)]
+
+
+class _PointSets(ctypes.Structure):
+    _fields_ = [("xyz", ctypes.POINTER(ctypes.c_double)), ("set_offsets", ctypes.POINTER(_I64)),
+                ("dropped", ctypes.POINTER(_I64)), ("n_sets", _INT)]
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 
@@ -193,6 +207,21 @@ def library() -> ctypes.CDLL:
     lib.d3g_gen_sphere.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, _I32, _P]
     lib.d3g_gen_clusters.argtypes = [_I64, ctypes.c_uint32, _I32, ctypes.c_double, _P]
     lib.d3g_gen_lattice.argtypes = [_I64, _P]
+    for name in ("d3g_mesh_load", "d3g_read_xyz"):
+        getattr(lib, name).argtypes = [ctypes.c_char_p, ctypes.POINTER(_Mesh)]
+        getattr(lib, name).restype = _INT
+    lib.d3g_mesh_weld.argtypes = [ctypes.POINTER(_Mesh)]
+    lib.d3g_mesh_weld.restype = _INT
+    lib.d3g_mesh_drop_non_finite.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_I64)]
+    lib.d3g_mesh_drop_non_finite.restype = _INT
+    lib.d3g_mesh_free.argtypes = [ctypes.POINTER(_Mesh)]
+    lib.d3g_mesh_free.restype = None
+    lib.d3g_mesh_supported_formats.argtypes = []
+    lib.d3g_mesh_supported_formats.restype = ctypes.c_char_p
+    lib.d3g_load_point_sets.argtypes = [ctypes.POINTER(ctypes.c_char_p), _INT, _INT, ctypes.POINTER(_PointSets)]
+    lib.d3g_load_point_sets.restype = _INT
+    lib.d3g_point_sets_free.argtypes = [ctypes.POINTER(_PointSets)]
+    lib.d3g_point_sets_free.restype = None
     for name in ("d3g_predicates", "d3g_predicates_device", "d3g_orient2d", "d3g_spatial_sort",
                  "d3g_spatial_sort_device", "d3g_shuffle_device", "d3g_build", "d3g_build_device"):
         getattr(lib, name).restype = _INT
@@ -734,3 +763,97 @@ def mixed_workload(n_sets: int, lo: int = 32, hi: int = 65536, seed: int = 2024,
     sizes = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), n_sets))).astype(np.int64)
     dists = rng.integers(0, len(DISTRIBUTIONS), n_sets)
     return [gen_set(DISTRIBUTIONS[d], int(n), first_seed + k) for k, (n, d) in enumerate(zip(sizes, dists))]
+
+
+# ---- input readers (host) -------------------------------------------------------------
+
+
+def _mesh_arrays(m: "_Mesh"):
+    v = np.ctypeslib.as_array(m.vertices, shape=(int(m.n_vertices) * 3,)).reshape(-1, 3).copy() \
+        if m.n_vertices else np.zeros((0, 3), dtype=np.float64)
+    f = np.ctypeslib.as_array(m.faces, shape=(int(m.n_faces) * 3,)).reshape(-1, 3).copy() \
+        if m.n_faces else np.zeros((0, 3), dtype=np.int32)
+    return v, f
+
+
+def _path_bytes(path) -> bytes:
+    return os.fsencode(path)
+
+
+def load_mesh(path):
+    """The reference viewer's reader (meshio::load, viewer/mesh_io.h:26-38): the
+    format by extension - .obj, .off, .ply, .stl (welded), .xyz/.txt/.pts or
+    none.  Returns (vertices (n, 3) float64, faces (m, 3) int32); raises
+    Del3dError with the reference's error text when the reader fails."""
+    lib = library()
+    m = _Mesh()
+    st = lib.d3g_mesh_load(_path_bytes(path), ctypes.byref(m))
+    try:
+        _check(st, "load_mesh")
+        return _mesh_arrays(m)
+    finally:
+        lib.d3g_mesh_free(ctypes.byref(m))
+
+
+def read_xyz(path) -> np.ndarray:
+    """examples/simple.cpp:17-23: "x y z" triples until the first that does not
+    parse; (n, 3) float64."""
+    lib = library()
+    m = _Mesh()
+    st = lib.d3g_read_xyz(_path_bytes(path), ctypes.byref(m))
+    try:
+        _check(st, "read_xyz")
+        return _mesh_arrays(m)[0]
+    finally:
+        lib.d3g_mesh_free(ctypes.byref(m))
+
+
+def _mesh_in(vertices, faces):
+    v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3).copy()
+    f = np.ascontiguousarray(faces if faces is not None else np.zeros((0, 3)), dtype=np.int32).reshape(-1, 3).copy()
+    m = _Mesh(v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), f.ctypes.data_as(ctypes.POINTER(_I32)),
+              v.shape[0], f.shape[0])
+    return v, f, m
+
+
+def weld(vertices, faces=None):
+    """meshio::weld: merges vertices with equal coordinates (first kept), remaps
+    the faces and drops faces whose corners merged.  Returns (vertices, faces)."""
+    v, f, m = _mesh_in(vertices, faces)
+    _check(library().d3g_mesh_weld(ctypes.byref(m)), "weld")
+    return v[:m.n_vertices].copy(), f[:m.n_faces].copy()
+
+
+def drop_non_finite(vertices, faces=None):
+    """meshio::drop_non_finite: removes vertices with a non-finite coordinate and
+    the faces touching them.  Returns (vertices, faces, dropped)."""
+    v, f, m = _mesh_in(vertices, faces)
+    d = _I64(0)
+    _check(library().d3g_mesh_drop_non_finite(ctypes.byref(m), ctypes.byref(d)), "drop_non_finite")
+    return v[:m.n_vertices].copy(), f[:m.n_faces].copy(), d.value
+
+
+def supported_formats() -> str:
+    return library().d3g_mesh_supported_formats().decode()
+
+
+def load_point_sets(paths, threads: int = 0):
+    """Reads many files as point sets on host threads (faces ignored, non-finite
+    vertices dropped) for a batched build.  Returns (xyz (N, 3) float64 with the
+    sets back to back, set_offsets (n + 1,) int64, dropped (n,) int64); the sets
+    are ``np.split(xyz, set_offsets[1:-1])``."""
+    lib = library()
+    enc = [_path_bytes(p) for p in paths]
+    arr = (ctypes.c_char_p * max(len(enc), 1))(*enc)
+    ps = _PointSets()
+    _check(lib.d3g_load_point_sets(arr, len(enc), int(threads), ctypes.byref(ps)), "load_point_sets")
+    try:
+        n = int(ps.n_sets)
+        offs = np.ctypeslib.as_array(ps.set_offsets, shape=(n + 1,)).copy()
+        total = int(offs[-1])
+        xyz = np.ctypeslib.as_array(ps.xyz, shape=(total * 3,)).reshape(-1, 3).copy() \
+            if total else np.zeros((0, 3), dtype=np.float64)
+        dropped = np.ctypeslib.as_array(ps.dropped, shape=(n,)).copy() if n else np.zeros(0, dtype=np.int64)
+        return xyz, offs, dropped
+    finally:
+        lib.d3g_point_sets_free(ctypes.byref(ps))

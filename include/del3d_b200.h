@@ -345,6 +345,53 @@ int d3g_reset_tuning(void);
  * independent chains per thread.  No counterpart in the reference. */
 int d3g_microbench_fp64(int64_t iters, double* addmul_ops_per_s, double* fma_per_s, void* stream);
 
+/* ---- input readers (host) -------------------------------------------------------
+ * The point and mesh formats of the reference's viewer reader (replaces
+ * meshio::load / weld / drop_non_finite / supported_formats,
+ * viewer/mesh_io.h:26-60): chosen by extension - .obj (Wavefront, polygons as
+ * fans, v/vt/vn and negative indices), .off (OFF/COFF/NOFF), .ply (ASCII and
+ * binary little-endian), .stl (ASCII and binary, welded), .xyz .txt .pts or no
+ * extension ("x y z" per line).  Vertices, faces and error texts equal the
+ * reference reader's on the same bytes.  No device is needed. */
+typedef struct d3g_mesh {
+    double* vertices;       /* n_vertices x 3 (x y z) */
+    int32_t* faces;         /* n_faces x 3 vertex indices (empty for a point set) */
+    int64_t n_vertices;
+    int64_t n_faces;
+} d3g_mesh;
+
+/* Loads `path`.  On a reader error returns D3G_ERR_INVALID_INPUT with the
+ * reference's text in d3g_last_error(); `out` then holds what was read before
+ * the error, as the reference's Mesh does.  Free with d3g_mesh_free. */
+int d3g_mesh_load(const char* path, d3g_mesh* out);
+/* examples/simple.cpp:17-23: "x y z" triples, whitespace-separated, until the
+ * first that does not parse. */
+int d3g_read_xyz(const char* path, d3g_mesh* out);
+/* In place: merges vertices with equal coordinates (the first kept, faces
+ * remapped, faces whose corners merged removed); nothing changes when no two
+ * vertices are equal.  A vertex with a NaN coordinate never merges. */
+int d3g_mesh_weld(d3g_mesh* m);
+/* In place: removes vertices with a non-finite coordinate and every face that
+ * touches one; `dropped` (may be NULL) receives how many vertices went. */
+int d3g_mesh_drop_non_finite(d3g_mesh* m, int64_t* dropped);
+void d3g_mesh_free(d3g_mesh* m);
+/* "obj, off, ply, stl, xyz". */
+const char* d3g_mesh_supported_formats(void);
+
+/* Many files as point sets for d3g_build_batch: every file is read (as
+ * d3g_mesh_load) on `threads` host threads (<= 0: one per core), its faces
+ * ignored and its non-finite vertices dropped (the build needs finite input),
+ * and the vertices packed back to back into pinned host memory.  A file that
+ * fails to read fails the call (D3G_ERR_INVALID_INPUT, "path: text"). */
+typedef struct d3g_point_sets {
+    double* xyz;            /* 3 doubles per point, set s at [set_offsets[s], set_offsets[s+1]) */
+    int64_t* set_offsets;   /* n_sets + 1 */
+    int64_t* dropped;       /* per set: non-finite vertices removed */
+    int n_sets;
+} d3g_point_sets;
+int d3g_load_point_sets(const char* const* paths, int n_paths, int threads, d3g_point_sets* out);
+void d3g_point_sets_free(d3g_point_sets* s);
+
 #ifdef __cplusplus
 }
 #endif

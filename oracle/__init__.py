@@ -12,7 +12,10 @@ Two libraries are loaded through ctypes:
   Bowyer-Watson build, canonical cell order);
 * ``_ref/libdel3d_ref.so`` -- the reference del3d compiled from its own sources
   (``oracle/Makefile``) plus its integer oracle ``tests/exact.h`` and its test
-  point-set generators ``tests/pointsets.h``.
+  point-set generators ``tests/pointsets.h``;
+* ``_ref/libmeshio_ref.so`` -- the reference viewer's mesh reader
+  (``viewer/mesh_io.cpp``) compiled from its source, the checker of the input
+  readers.
 """
 from __future__ import annotations
 
@@ -26,8 +29,11 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _ORC_PATH = os.path.join(_HERE, "liboracle.so")
 _REF_PATH = os.path.join(_HERE, "_ref", "libdel3d_ref.so")
 
+_MESHIO_PATH = os.path.join(_HERE, "_ref", "libmeshio_ref.so")
+
 _orc: Optional[ctypes.CDLL] = None
 _ref: Optional[ctypes.CDLL] = None
+_meshio: Optional[ctypes.CDLL] = None
 
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
@@ -299,3 +305,82 @@ def ps_rng_below(seed: int, m: int, count: int) -> np.ndarray:
     out = np.zeros(count, dtype=np.int64)
     ref().ps_rng_below(seed, m, count, _ptr(out))
     return out
+
+
+# ---- the reference viewer's mesh reader ------------------------------------------------
+
+
+class _RefMesh(ctypes.Structure):
+    _fields_ = [("v", ctypes.POINTER(ctypes.c_double)), ("f", ctypes.POINTER(ctypes.c_int32)),
+                ("nv", _I64), ("nf", _I64), ("err", ctypes.c_char * 512)]
+
+
+def ref_meshio_available() -> bool:
+    return os.path.exists(_MESHIO_PATH)
+
+
+def _meshio_lib() -> ctypes.CDLL:
+    global _meshio
+    if _meshio is None:
+        lib = ctypes.CDLL(_MESHIO_PATH)
+        lib.ref_mesh_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(_RefMesh)]
+        lib.ref_mesh_load.restype = _INT
+        lib.ref_mesh_weld.argtypes = [_P, _I64, _P, _I64, ctypes.POINTER(_RefMesh)]
+        lib.ref_mesh_weld.restype = None
+        lib.ref_mesh_drop_non_finite.argtypes = [_P, _I64, _P, _I64, ctypes.POINTER(_RefMesh)]
+        lib.ref_mesh_drop_non_finite.restype = _I64
+        lib.ref_mesh_free.argtypes = [ctypes.POINTER(_RefMesh)]
+        lib.ref_mesh_formats.restype = ctypes.c_char_p
+        _meshio = lib
+    return _meshio
+
+
+def _ref_arrays(m: _RefMesh):
+    v = np.ctypeslib.as_array(m.v, shape=(int(m.nv) * 3,)).reshape(-1, 3).copy() if m.nv \
+        else np.zeros((0, 3), dtype=np.float64)
+    f = np.ctypeslib.as_array(m.f, shape=(int(m.nf) * 3,)).reshape(-1, 3).copy() if m.nf \
+        else np.zeros((0, 3), dtype=np.int32)
+    return v, f
+
+
+def ref_mesh_load(path):
+    """meshio::load of the reference: (vertices, faces, error text or "")."""
+    lib = _meshio_lib()
+    m = _RefMesh()
+    lib.ref_mesh_load(os.fsencode(path), ctypes.byref(m))
+    try:
+        v, f = _ref_arrays(m)
+        return v, f, m.err.decode()
+    finally:
+        lib.ref_mesh_free(ctypes.byref(m))
+
+
+def ref_weld(v, f):
+    """meshio::weld of the reference: (vertices, faces)."""
+    lib = _meshio_lib()
+    v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+    f = np.ascontiguousarray(f, dtype=np.int32).reshape(-1, 3)
+    m = _RefMesh()
+    lib.ref_mesh_weld(_ptr(v), v.shape[0], _ptr(f), f.shape[0], ctypes.byref(m))
+    try:
+        return _ref_arrays(m)
+    finally:
+        lib.ref_mesh_free(ctypes.byref(m))
+
+
+def ref_drop_non_finite(v, f):
+    """meshio::drop_non_finite of the reference: (vertices, faces, dropped)."""
+    lib = _meshio_lib()
+    v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+    f = np.ascontiguousarray(f, dtype=np.int32).reshape(-1, 3)
+    m = _RefMesh()
+    d = lib.ref_mesh_drop_non_finite(_ptr(v), v.shape[0], _ptr(f), f.shape[0], ctypes.byref(m))
+    try:
+        vv, ff = _ref_arrays(m)
+        return vv, ff, int(d)
+    finally:
+        lib.ref_mesh_free(ctypes.byref(m))
+
+
+def ref_mesh_formats() -> str:
+    return _meshio_lib().ref_mesh_formats().decode()
