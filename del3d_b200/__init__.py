@@ -238,7 +238,7 @@ def _status_string(status: int) -> str:
 
 def _check(status: int, where: str) -> None:
     if status != 0:
-        detail = library().d3g_last_error().decode()
+        detail = library().d3g_last_error().decode(errors="replace")   # may quote file bytes
         raise Del3dError(status, where, detail)
 
 

@@ -463,6 +463,9 @@ void read_ply(Cursor& in, Mesh& m, std::string& err) {
             err = "PLY vertex element has no x/y/z";
             return;
         }
+        // A binary element without properties occupies no bytes: its items change
+        // nothing, however many the header claims (the reference walks them all).
+        if (!ascii && e.props.empty()) continue;
         for (long n = 0; n < e.count; ++n) {
             scalars.assign(e.props.size(), 0.0);
             poly.clear();

@@ -331,6 +331,7 @@ def _meshio_lib() -> ctypes.CDLL:
         lib.ref_mesh_drop_non_finite.restype = _I64
         lib.ref_mesh_free.argtypes = [ctypes.POINTER(_RefMesh)]
         lib.ref_mesh_formats.restype = ctypes.c_char_p
+        lib.ref_mesh_error.restype = ctypes.c_char_p
         _meshio = lib
     return _meshio
 
@@ -343,14 +344,17 @@ def _ref_arrays(m: _RefMesh):
     return v, f
 
 
-def ref_mesh_load(path):
-    """meshio::load of the reference: (vertices, faces, error text or "")."""
+def ref_mesh_load(path, with_status=False):
+    """meshio::load of the reference: (vertices, faces, error text or "").  The
+    text is decoded with surrogateescape (it may quote bytes of the file).  With
+    `with_status`, also 2 when the reference threw (it would abort a program)."""
     lib = _meshio_lib()
     m = _RefMesh()
-    lib.ref_mesh_load(os.fsencode(path), ctypes.byref(m))
+    rc = lib.ref_mesh_load(os.fsencode(path), ctypes.byref(m))
     try:
         v, f = _ref_arrays(m)
-        return v, f, m.err.decode()
+        err = lib.ref_mesh_error().decode(errors="surrogateescape")
+        return (v, f, err, rc) if with_status else (v, f, err)
     finally:
         lib.ref_mesh_free(ctypes.byref(m))
 

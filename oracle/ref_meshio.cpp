@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <string>
 
 extern "C" {
@@ -48,15 +49,29 @@ void ref_mesh_free(RefMesh* m) {
     m->nv = m->nf = 0;
 }
 
-/// meshio::load; returns 1 when it set an error (text in out->err).
+static thread_local std::string g_err;
+
+/// meshio::load; returns 1 when it set an error (full text from
+/// ref_mesh_error, the first 511 bytes also in out->err), 2 when it threw (the
+/// reference aborts a program on such a file, e.g. a count it cannot reserve).
 int ref_mesh_load(const char* path, RefMesh* out) {
-    std::string err;
-    const meshio::Mesh m = meshio::load(path, err);
+    int rc = 0;
+    meshio::Mesh m;
+    try {
+        g_err.clear();
+        m = meshio::load(path, g_err);
+        rc = g_err.empty() ? 0 : 1;
+    } catch (const std::exception& e) {
+        g_err = std::string("threw: ") + e.what();
+        rc = 2;
+    }
     to_c(m, out);
-    std::strncpy(out->err, err.c_str(), sizeof out->err - 1);
+    std::strncpy(out->err, g_err.c_str(), sizeof out->err - 1);
     out->err[sizeof out->err - 1] = '\0';
-    return err.empty() ? 0 : 1;
+    return rc;
 }
+
+const char* ref_mesh_error() { return g_err.c_str(); }
 
 /// meshio::weld of the given arrays, result in `out`.
 void ref_mesh_weld(const double* v, int64_t nv, const int32_t* f, int64_t nf, RefMesh* out) {

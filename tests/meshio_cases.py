@@ -82,6 +82,9 @@ def hand_cases():
     c["no_vertices.ply"] = b"ply\nformat ascii 1.0\nelement vertex 0\nproperty float x\nproperty float y\nproperty float z\nend_header\n"
     c["header_only.ply"] = b"ply\nformat ascii 1.0\nelement vertex\nproperty\nproperty list\nelement face abc\nend_header\n"
     c["binary.ply"] = binary_ply(np.random.default_rng(1), 40, 20)
+    c["binary_empty_element.ply"] = (b"ply\nformat binary_little_endian 1.0\nelement marker 5\n"
+                                     b"element vertex 1\nproperty double x\nproperty double y\n"
+                                     b"property double z\nend_header\n" + struct.pack("<3d", 1, 2, 3))
     c["binary_truncated.ply"] = binary_ply(np.random.default_rng(2), 10, 5)[:-7]
     c["binary_unknown_type.ply"] = (b"ply\nformat binary_little_endian 1.0\nelement vertex 1\n"
                                     b"property float x\nproperty float y\nproperty float z\nproperty half w\n"
@@ -282,3 +285,31 @@ def write_cases(root, cases):
             f.write(data)
         paths.append(p)
     return paths
+
+
+def mutated_cases(n, seed):
+    """Byte-level mutations of the cases above (flips to separators and number
+    characters, cuts, inserted text and tokens): malformed files of every kind."""
+    rng = np.random.default_rng(seed)
+    items = list({**hand_cases(), **random_cases(8, 3)}.items())
+    toks = [b"12", b"-1", b"1e3", b" \n", b"nan", b"0.5", b"\r\n", b"#"]
+    out = {}
+    for it in range(n):
+        name, data = items[int(rng.integers(0, len(items)))]
+        b = bytearray(data)
+        for _ in range(int(rng.integers(1, 4))):
+            op = int(rng.integers(0, 4))
+            if op == 0 and b:
+                b[int(rng.integers(0, len(b)))] = int(rng.choice([32, 10, 13, 9, 46, 45, 43, 101, 48, 49, 35, 47, 0,
+                                                                  255, int(rng.integers(0, 256))]))
+            elif op == 1 and b:
+                i = int(rng.integers(0, len(b)))
+                del b[i:i + int(rng.integers(1, 10))]
+            elif op == 2:
+                i = int(rng.integers(0, len(b) + 1))
+                b[i:i] = bytes(rng.integers(32, 127, int(rng.integers(1, 6))).astype(np.uint8))
+            else:
+                i = int(rng.integers(0, len(b) + 1))
+                b[i:i] = toks[int(rng.integers(0, len(toks)))]
+        out[f"m{it}_{name.replace('/', '_')}"] = bytes(b)
+    return out
