@@ -576,14 +576,47 @@ void read_stl_ascii(Cursor& in, Mesh& m, std::string& err) {
 
 // ---- "x y z" text (viewer/mesh_io.cpp:402-413) -------------------------------------
 
-void read_xyz_lines(Cursor& in, Mesh& m, std::string& err) {
+void xyz_lines(string_view text, std::vector<double>& v) {
+    Cursor in(text), ls;
     string_view ln;
-    Cursor ls;
     while (in.line(ln)) {
         if (ln.empty() || ln[0] == '#') continue;
         ls.reset(ln);
         double x, y, z;
-        if (ls.number(x) && ls.number(y) && ls.number(z)) m.vertex(x, y, z);
+        if (ls.number(x) && ls.number(y) && ls.number(z)) {
+            v.push_back(x);
+            v.push_back(y);
+            v.push_back(z);
+        }
+    }
+}
+
+/// Lines are read independently, so a large file is cut at line starts into
+/// one piece per thread and the pieces' points are joined in order: the same
+/// points as one pass.
+void read_xyz_lines(string_view text, Mesh& m, std::string& err, int threads) {
+    constexpr size_t kMinPiece = size_t(2) << 20;
+    const int nt = int(std::min<size_t>(size_t(std::max(threads, 1)), text.size() / kMinPiece + 1));
+    if (nt <= 1) {
+        xyz_lines(text, m.v);
+    } else {
+        std::vector<size_t> cut(size_t(nt) + 1, text.size());
+        cut[0] = 0;
+        for (int t = 1; t < nt; ++t) {
+            size_t pos = std::max(cut[size_t(t) - 1], text.size() / size_t(nt) * size_t(t));
+            const size_t nl = text.find('\n', pos);
+            cut[size_t(t)] = nl == string_view::npos ? text.size() : nl + 1;
+        }
+        std::vector<std::vector<double>> part(static_cast<size_t>(nt));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t)
+            pool.emplace_back([&, t] { xyz_lines(text.substr(cut[size_t(t)], cut[size_t(t) + 1] - cut[size_t(t)]), part[size_t(t)]); });
+        xyz_lines(text.substr(0, cut[1]), part[0]);
+        for (std::thread& th : pool) th.join();
+        size_t total = 0;
+        for (const auto& p : part) total += p.size();
+        m.v.reserve(total);
+        for (const auto& p : part) m.v.insert(m.v.end(), p.begin(), p.end());
     }
     if (m.v.empty()) err = "no points in the file";
 }
@@ -707,8 +740,12 @@ std::string extension(const std::string& path) {
 
 const char* kFormats = "obj, off, ply, stl, xyz";
 
-/// meshio::load: the reader by extension; `err` empty on success.
-void load_mesh(const std::string& path, Mesh& m, std::string& err) {
+int host_threads() { return int(std::max(1u, std::thread::hardware_concurrency())); }
+
+/// meshio::load: the reader by extension; `err` empty on success.  `threads`
+/// parse a large "x y z" text file in pieces (the other formats are read in
+/// one pass: their items depend on what came before).
+void load_mesh(const std::string& path, Mesh& m, std::string& err, int threads) {
     err.clear();
     std::vector<char> buf;
     if (!read_file(path.c_str(), buf)) {
@@ -731,7 +768,7 @@ void load_mesh(const std::string& path, Mesh& m, std::string& err) {
         m.v.resize(size_t(nv) * 3);
         m.f.resize(size_t(nf) * 3);
     } else if (ext == ".xyz" || ext == ".txt" || ext == ".pts" || ext.empty()) {
-        read_xyz_lines(in, m, err);
+        read_xyz_lines(string_view(buf.data(), buf.size()), m, err, threads);
     } else {
         err = "unknown extension '" + ext + "' (" + kFormats + ")";
     }
@@ -762,7 +799,7 @@ namespace meshio {
 
 Mesh load(const std::string& path, std::string& error) {
     ::Mesh m;
-    load_mesh(path, m, error);
+    load_mesh(path, m, error, host_threads());
     Mesh r;
     r.vertices.resize(m.nv());
     if (!m.v.empty()) std::memcpy(r.vertices.data(), m.v.data(), m.v.size() * sizeof(double));
@@ -818,7 +855,7 @@ static int d3g_mesh_load_impl(const char* path, d3g_mesh* out) {
     *out = d3g_mesh{};
     Mesh m;
     std::string err;
-    load_mesh(path, m, err);
+    load_mesh(path, m, err, host_threads());
     const int st = fill_mesh(m, out);
     if (st != D3G_OK) return st;
     if (!err.empty()) {
@@ -904,14 +941,15 @@ static int d3g_load_point_sets_impl(const char* const* paths, int n_paths, int t
     std::vector<Mesh> meshes(static_cast<size_t>(n_paths));
     std::vector<std::string> errs(static_cast<size_t>(n_paths));
     std::vector<int64_t> dropped(size_t(n_paths), 0);
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int nt = std::max(1, std::min(n_paths, threads > 0 ? threads : int(hw)));
+    const int want = threads > 0 ? threads : host_threads();
+    const int nt = std::max(1, std::min(n_paths, want));
+    const int per_file = std::max(1, want / std::max(n_paths, 1));   // few large files: split them too
     std::atomic<int> next{0};
     auto work = [&]() {
         for (int i; (i = next.fetch_add(1)) < n_paths;) {
             Mesh& m = meshes[size_t(i)];
             try {
-                load_mesh(paths[i], m, errs[size_t(i)]);
+                load_mesh(paths[i], m, errs[size_t(i)], per_file);
                 m.f.clear();
                 int64_t nv = int64_t(m.nv()), nf = 0;
                 dropped[size_t(i)] = drop_non_finite_arrays(m.v.data(), nv, nullptr, nf);

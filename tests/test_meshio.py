@@ -103,6 +103,26 @@ def test_mutated_files_match_reference(tmp_path):
 
 
 @needs_ref
+def test_large_xyz_in_pieces_matches_reference(tmp_path):
+    """A text file above the piece size is parsed by several threads, cut at
+    line starts; the points must be those of one pass."""
+    rng = np.random.default_rng(31)
+    chunks = [mc.random_xyz(rng) for _ in range(6000)]
+    data = b"".join(chunks)
+    big = b""
+    while len(big) < (9 << 20):
+        big += data
+    p = str(tmp_path / "big.xyz")
+    with open(p, "wb") as fh:
+        fh.write(big)
+    ours, ref = ours_raw(p), oracle.ref_mesh_load(p)
+    assert ours[0].shape[0] > 100_000
+    assert same(ours, ref)
+    xyz, offs, _ = d3.load_point_sets([p], threads=4)      # one file, split four ways
+    assert np.array_equal(xyz.view(np.uint64), d3.drop_non_finite(ref[0], None)[0].view(np.uint64))
+
+
+@needs_ref
 def test_missing_file_matches_reference(tmp_path):
     p = str(tmp_path / "absent.obj")
     assert same(ours_raw(p), oracle.ref_mesh_load(p))
