@@ -316,7 +316,13 @@ class _RefMesh(ctypes.Structure):
 
 
 def ref_meshio_available() -> bool:
-    return os.path.exists(_MESHIO_PATH)
+    """Built, and linked against the shared C++ runtime (a copy of libstdc++
+    linked in statically breaks its streams in a process that loaded the shared
+    one, as numpy does)."""
+    if not os.path.exists(_MESHIO_PATH):
+        return False
+    with open(_MESHIO_PATH, "rb") as fh:
+        return b"libstdc++.so.6" in fh.read()
 
 
 def _meshio_lib() -> ctypes.CDLL:
