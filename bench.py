@@ -39,6 +39,13 @@ the device default; the line reports the choice under "tuning".
 
 `--impl reference` times the reference's own CPU build on the same sample
 (rank 0 only; all host threads, one set per thread).
+
+`--workload readers` (host only, no GPU): every 16th set of the batched workload
+written to files in turn as "x y z" text, binary PLY, OBJ and OFF; a step reads
+them all with d3g_load_point_sets (all host threads) into the back-to-back layout
+of a batched build; cpu_baseline is the reference viewer's reader
+(viewer/mesh_io.cpp, compiled from source) on the same files with the same
+threads, and the line says whether the points read are the reference's.
 """
 from __future__ import annotations
 
@@ -73,10 +80,12 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "plain", "predicates", "sort"],
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "plain", "predicates", "sort", "readers"],
                     help="batched: the headline line; plain: one single-set build per step "
                          "(--n uniform points); predicates / sort: the predicate and "
-                         "spatial-sort microbenchmarks, one line each")
+                         "spatial-sort microbenchmarks, one line each; readers: the host "
+                         "input readers on files of a sample of the batched sets (no GPU)")
     ap.add_argument("--n", type=int, default=PLAIN_N, help="points of the plain workload")
     ap.add_argument("--dist", default="uniform", choices=["uniform", "clusters", "lattice", "sphere"],
                     help="distribution of the plain workload")
@@ -860,8 +869,93 @@ def run_sort(args):
     return 0
 
 
+READER_EVERY = 16
+
+
+def _write_reader_files(root, sets):
+    """Set k goes to a file in format k % 4: text, binary PLY, OBJ, OFF."""
+    import numpy as np
+
+    paths = []
+    for k, pts in enumerate(sets):
+        fmt = k % 4
+        if fmt == 0:
+            p = os.path.join(root, f"s{k}.xyz")
+            np.savetxt(p, pts, fmt="%.17g")
+        elif fmt == 1:
+            p = os.path.join(root, f"s{k}.ply")
+            hdr = (f"ply\nformat binary_little_endian 1.0\nelement vertex {pts.shape[0]}\n"
+                   "property double x\nproperty double y\nproperty double z\nend_header\n").encode()
+            with open(p, "wb") as fh:
+                fh.write(hdr + np.ascontiguousarray(pts, dtype="<f8").tobytes())
+        elif fmt == 2:
+            p = os.path.join(root, f"s{k}.obj")
+            np.savetxt(p, pts, fmt="v %.17g %.17g %.17g")
+        else:
+            p = os.path.join(root, f"s{k}.off")
+            np.savetxt(p, pts, fmt="%.17g", header=f"OFF\n{pts.shape[0]} 0 0", comments="")
+        paths.append(p)
+    return paths
+
+
+def run_readers(args):
+    import shutil
+    import tempfile
+
+    import numpy as np
+
+    import del3d_b200 as d3
+
+    threads = os.cpu_count() or 1
+    sets = workload_sets(args.sets, 0)[::READER_EVERY]
+    root = tempfile.mkdtemp(prefix="d3g_readers_")
+    try:
+        paths = _write_reader_files(root, sets)
+        n_points = sum(int(a.shape[0]) for a in sets)
+        mb = sum(os.path.getsize(p) for p in paths) / 1e6
+        for _ in range(args.warmup):
+            d3.load_point_sets(paths, threads=threads)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            xyz, offs, dropped = d3.load_point_sets(paths, threads=threads)
+        dt = (time.perf_counter() - t0) / args.steps
+        line = {"metric": "input reader points/s (files to back-to-back host points)",
+                "value": n_points / dt, "unit": "points/s", "n_gpus": 0, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": f"every {READER_EVERY}th set of the batched workload ({len(sets)} sets, "
+                                       f"{n_points} points, {mb:.0f} MB) as files, formats in turn: x y z "
+                                       "text, binary little-endian PLY, OBJ, OFF", "threads": threads},
+                "sets_equal_input": bool(all(np.array_equal(xyz[offs[k]:offs[k + 1]], a)
+                                             for k, a in enumerate(sets)))}
+        try:
+            import oracle
+
+            ref_ok = oracle.ref_meshio_available()
+        except ImportError:
+            ref_ok = False
+        if ref_ok and not args.no_cpu_baseline:
+            with ThreadPoolExecutor(threads) as ex:
+                t0 = time.perf_counter()
+                ref = list(ex.map(oracle.ref_mesh_load, paths))
+                t = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": n_points / t, "unit": "points/s", "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"the same {len(paths)} files, one reader call per file on "
+                                              f"{threads} host threads ({t:.2f} s)"}
+            line["equals_reference"] = bool(all(
+                np.array_equal(xyz[offs[k]:offs[k + 1]].view(np.uint64), r[0].view(np.uint64)) and not r[2]
+                for k, r in enumerate(ref)))
+        print(json.dumps(line))
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.workload == "readers":
+        return run_readers(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "predicates":

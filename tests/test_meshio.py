@@ -255,3 +255,15 @@ def test_cpp_dropin_header_builds_and_runs(tmp_path):
     mesh = mc.write_cases(str(tmp_path), {"cube.off": mc.hand_cases()["cube.off"]})[0]
     out = subprocess.run([str(exe), mesh], capture_output=True, text=True, timeout=60)
     assert out.returncode == 0 and out.stdout.strip() == "8 12 0 |obj, off, ply, stl, xyz", out.stdout
+
+
+def test_bench_readers_workload_line():
+    """bench.py --workload readers (host only) prints one JSON line whose points
+    are the input's and, where the reference reader is built, the reference's."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--workload", "readers", "--sets", "64",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["unit"] == "points/s" and line["value"] > 0 and line["sets_equal_input"]
+    if oracle.ref_meshio_available():
+        assert line["equals_reference"] and line["cpu_baseline"]["kind"] == "reference"
