@@ -106,6 +106,22 @@ def parse_args():
     return ap.parse_args()
 
 
+def job_rate(dist, device, units, seconds):
+    """Whole-job rate over the ranks: the units all ranks processed (their sets
+    differ in size) over the slowest rank's time.  Every rank calls it at the
+    same point, in the same order (two collectives).  Returns (rate, max
+    seconds, total units)."""
+    import torch
+
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    t_max, total = float(t.item()), float(u.item())
+    return total / t_max, t_max, total
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -487,11 +503,9 @@ def run_ours(args):
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * n / (ms_max / 1000.0)
+    value, s_max, _ = job_rate(dist, dev, n, ms / 1000.0)
+    tets_rate, _, _ = job_rate(dist, dev, ncells, ms / 1000.0)
+    ms_max = s_max * 1000.0
 
     if args.profile_run:
         if rank == 0:
@@ -535,10 +549,7 @@ def run_ours(args):
         for _ in range(args.steps):
             e2e_cells = e2e_call()
         t_e2e = (time.perf_counter() - t0) / args.steps
-        te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_value = world * n / float(te.item())
+        e2e_value, _, _ = job_rate(dist, dev, n, t_e2e)
 
     # ---- the plain one-set-per-call path on a sample of the same sets ----
     plain = None
@@ -592,7 +603,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config(len(sets), n),
-            "tets_per_s": world * ncells / (ms_max / 1000.0),
+            "tets_per_s": tets_rate,
             "e2e": ({"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": 24 * n,
                      "d2h_bytes_per_step": 16 * int(e2e_cells) + 16 * len(sets) + 8}
                     if e2e_value else None),
