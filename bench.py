@@ -25,6 +25,9 @@ One JSON line (rank 0):
               (live counts) / its event-timed duration, against measured HBM;
   cpu_baseline  the reference del3d compiled from source on a 1-in-16 sample of
               the sets, one set per host thread.
+  parity      the checker: the timed build's cells of every 64th set against
+              the reference's build of the same set in canonical order; the run
+              exits 1 when they differ.
   plain_1e7   the plain path on 1e7 uniform points and the reference's
               single-threaded build rate on 1e6 of them.
   serving     the request server (d3g_server_*, continuous batching, admission
@@ -271,6 +274,34 @@ def cpu_baseline_leg(sets):
                       f"({pts / cpu_s:.0f} points/s per thread)"}
 
 
+PARITY_EVERY = 64
+
+
+def parity_leg(sets, gpu_cells):
+    """The checker: the cells the timed batched build gave every PARITY_EVERY-th
+    set (`gpu_cells`: set index -> host array) against the reference's build of
+    that set (oracle/_ref), put in the same canonical order; one set per host
+    thread.  None when the reference library is absent."""
+    import numpy as np
+
+    import oracle
+
+    if not oracle.ref_available() or not gpu_cells:
+        return None
+
+    def one(k):
+        want = oracle.canonical_cells(oracle.ref_build(sets[k])["cells"])
+        return bool(np.array_equal(gpu_cells[k], want))
+
+    idx = sorted(gpu_cells)
+    with ThreadPoolExecutor(max_workers=host_threads()) as ex:
+        ok = list(ex.map(one, idx))
+    return {"sets": len(idx), "points": int(sum(sets[k].shape[0] for k in idx)), "equal": all(ok),
+            "mismatched_sets": [k for k, o in zip(idx, ok) if not o][:10],
+            "checker": "the reference build (oracle/_ref) of every "
+                       f"{PARITY_EVERY}th set, canonical order, against the timed build's cells"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -500,6 +531,10 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop() if clocks else None
+    # After the timed region: the cells of a sample of sets, for the parity check.
+    par_cells = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_run:
+        par_cells = {k: cells[int(co[k]):int(co[k + 1])].cpu().numpy() for k in range(0, len(sets), PARITY_EVERY)}
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1) / args.steps
@@ -631,11 +666,15 @@ def run_ours(args):
             line["serving"] = serving_leg(torch, d3)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_leg(sets)
+            line["parity"] = parity_leg(sets, par_cells)
     if rank == 0:
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0 and line.get("parity") and not line["parity"]["equal"]:
+        print("bench: the timed build's cells differ from the reference's", file=sys.stderr)
+        return 1
     return 0
 
 
