@@ -8,7 +8,9 @@ the unit sphere quantised to a 2^-10 grid (duplicates removed), float64, per-set
 seeds (del3d_b200.mixed_workload).  All sets go to the GPU in one batched build
 (d3g_build_batch_device); every set's tet set is the reference's.  With N > 1
 GPUs each rank builds its own 4096 sets (weak scaling, no exchange step: sets
-are independent).
+are independent); `--scaling strong` splits one 4096-set workload among the
+ranks by estimated cost instead (del3d_b200.partition_sets).  The whole-job
+rate is every rank's points over the slowest rank's time.
 
 One JSON line (rank 0):
   value       points/s of the whole job, inputs resident in HBM, device-timed
@@ -98,6 +100,10 @@ def parse_args():
                     help="plain workload: launch each round's kernels separately with event "
                          "timing (the form the ncu launch list captures)")
     ap.add_argument("--sets", type=int, default=N_SETS)
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="N > 1 GPUs: weak - every rank builds its own --sets sets (the default); "
+                         "strong - the ranks share one --sets workload, split by estimated cost "
+                         "(del3d_b200.partition_sets)")
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -137,6 +143,19 @@ def workload_sets(n_sets, rank):
     import del3d_b200 as d3
 
     return d3.mixed_workload(n_sets, LO, HI, seed=2024 + rank, first_seed=1000 + n_sets * rank)
+
+
+def rank_sets(n_sets, rank, world, scaling):
+    """The sets rank `rank` builds: its own n_sets sets (weak scaling), or its
+    share of one n_sets workload split by estimated cost (strong scaling; every
+    rank generates the same workload and keeps its part, so nothing is sent)."""
+    if scaling == "weak" or world == 1:
+        return workload_sets(n_sets, rank)
+    import del3d_b200 as d3
+
+    sets = workload_sets(n_sets, 0)
+    part = d3.partition_sets([a.shape[0] for a in sets], world)[rank]
+    return [sets[k] for k in part]
 
 
 def config(n_sets, n_points):
@@ -479,7 +498,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
 
     t_gen = time.perf_counter()
-    sets = workload_sets(args.sets, rank)
+    sets = rank_sets(args.sets, rank, world, args.scaling)
     t_gen = time.perf_counter() - t_gen
     sizes = np.array([a.shape[0] for a in sets], dtype=np.int64)
     offs = np.zeros(len(sets) + 1, dtype=np.int64)
@@ -636,8 +655,11 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config(len(sets), n),
+            "higher_is_better": True, "scaling": args.scaling if world > 1 else "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": dict(config(len(sets), n), **({"partition": f"{args.sets} sets split among {world} ranks "
+                                                                   "by estimated cost n log2 n"}
+                                                    if world > 1 and args.scaling == "strong" else {})),
             "tets_per_s": tets_rate,
             "e2e": ({"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": 24 * n,
                      "d2h_bytes_per_step": 16 * int(e2e_cells) + 16 * len(sets) + 8}

@@ -36,7 +36,7 @@ __all__ = [
     "collinear", "spatial_sort", "library", "LIB_PATH", "predicate_stats", "circumcenters",
     "circumcenter", "circumcenter_lazy", "Server", "Request", "pool_usage",
     "release_cached_memory", "load_mesh", "read_xyz", "weld", "drop_non_finite",
-    "supported_formats", "load_point_sets",
+    "supported_formats", "load_point_sets", "partition_sets",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -753,6 +753,34 @@ def gen_set(dist: str, n: int, seed: int) -> np.ndarray:
     if dist == "lattice":
         return gen_lattice(n)
     return gen_sphere(n, seed, 1.0, 1024, dedupe=True)
+
+
+def partition_sets(sizes, n_parts: int, weights=None) -> List[List[int]]:
+    """Splits independent point sets among `n_parts` GPUs (or streams) so that
+    their build costs balance: longest-first greedy on the estimated cost
+    n log2 n (times `weights[k]` if given - e.g. about 5 for integer lattices,
+    whose degenerate cospherical cells cost more), each set to the least loaded
+    part, ties to the lower part.  Deterministic; returns each part's set
+    indices in ascending order.  Sets are independent, so the parts need no
+    exchange step."""
+    import heapq
+
+    n_parts = int(n_parts)
+    if n_parts < 1:
+        raise ValueError("n_parts must be at least 1")
+    sizes = np.asarray(sizes, dtype=np.float64).reshape(-1)
+    w = np.ones_like(sizes) if weights is None else np.asarray(weights, dtype=np.float64).reshape(-1)
+    if w.shape != sizes.shape:
+        raise ValueError("weights must match sizes")
+    cost = sizes * np.log2(np.maximum(sizes, 2.0)) * w
+    order = np.argsort(-cost, kind="stable")
+    heap = [(0.0, p) for p in range(n_parts)]
+    parts: List[List[int]] = [[] for _ in range(n_parts)]
+    for k in order.tolist():
+        load, p = heapq.heappop(heap)
+        parts[p].append(k)
+        heapq.heappush(heap, (load + float(cost[k]), p))
+    return [sorted(part) for part in parts]
 
 
 def mixed_workload(n_sets: int, lo: int = 32, hi: int = 65536, seed: int = 2024, first_seed: int = 1000):
