@@ -27,7 +27,7 @@ One JSON line (rank 0):
               (live counts) / its event-timed duration, against measured HBM;
   cpu_baseline  the reference del3d compiled from source on a 1-in-16 sample of
               the sets, one set per host thread.
-  parity      the checker: the timed build's cells of every 64th set against
+  parity      the parity check: the timed build's cells of every 64th set against
               the reference's build of the same set in canonical order; the run
               exits 1 when they differ.
   plain_1e7   the plain path on 1e7 uniform points and the reference's
@@ -297,7 +297,7 @@ PARITY_EVERY = 64
 
 
 def parity_leg(sets, gpu_cells):
-    """The checker: the cells the timed batched build gave every PARITY_EVERY-th
+    """Parity: the cells the timed batched build gave every PARITY_EVERY-th
     set (`gpu_cells`: set index -> host array) against the reference's build of
     that set (oracle/_ref), put in the same canonical order; one set per host
     thread.  None when the reference library is absent."""
@@ -317,7 +317,7 @@ def parity_leg(sets, gpu_cells):
         ok = list(ex.map(one, idx))
     return {"sets": len(idx), "points": int(sum(sets[k].shape[0] for k in idx)), "equal": all(ok),
             "mismatched_sets": [k for k, o in zip(idx, ok) if not o][:10],
-            "checker": "the reference build (oracle/_ref) of every "
+            "method": "the reference build (oracle/_ref) of every "
                        f"{PARITY_EVERY}th set, canonical order, against the timed build's cells"}
 
 

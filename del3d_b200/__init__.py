@@ -676,7 +676,7 @@ def pool_usage(reset_high: bool = False):
 
 
 def release_cached_memory() -> None:
-    """Returns the cached device blocks and the pool's reserve to the driver and
+    """Returns the cached device blocks and the pool's reserve to the CUDA driver and
     unpins the cached host result blocks (synchronises the device)."""
     _check(library().d3g_release_cached_memory(), "release_cached_memory")
 

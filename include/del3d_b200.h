@@ -59,7 +59,7 @@ const char* d3g_last_error(void);
  * quarter of the device memory), the rest in the current device's stream-ordered
  * pool.  Host result arrays come from a cache of pinned blocks (freed results'
  * blocks serve later ones, up to 16 GiB).  This returns all of them to the
- * driver; it synchronises the device. */
+ * CUDA driver; it synchronises the device. */
 int d3g_release_cached_memory(void);
 
 /* ---- predicates ------------------------------------------------------------

@@ -1,8 +1,8 @@
-"""Parity checkers for the del3d ``Delaunay::build`` path.
+"""Parity oracles for the del3d ``Delaunay::build`` path.
 
 TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
 ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import this
-package, and only as the checker or the timed CPU baseline -- never as part of
+package, and only as the oracle or the timed CPU baseline -- never as part of
 the product path (``del3d_b200`` never imports it).
 
 Two libraries are loaded through ctypes:
@@ -14,7 +14,7 @@ Two libraries are loaded through ctypes:
   (``oracle/Makefile``) plus its integer oracle ``tests/exact.h`` and its test
   point-set generators ``tests/pointsets.h``;
 * ``_ref/libmeshio_ref.so`` -- the reference viewer's mesh reader
-  (``viewer/mesh_io.cpp``) compiled from its source, the checker of the input
+  (``viewer/mesh_io.cpp``) compiled from its source, the oracle of the input
   readers.
 """
 from __future__ import annotations
