@@ -15,6 +15,7 @@
  *   del3d::spatial_sort                                    include/del3d/spatial_sort.h:37
  *   del3d::Delaunay::build / finite_cells / all_cells /
  *     incident_cells / number_of_vertices                  include/del3d/delaunay.h:68-85
+ *   meshio::load / weld / drop_non_finite (viewer reader)  viewer/mesh_io.h:26-60
  *
  * Documented difference from the reference: finite_cells() comes back in a
  * canonical order instead of the reference's cell-allocation order.  Each tet
