@@ -15,10 +15,12 @@
 // extraction leaves the cursor failed, so every later read fails too.  The
 // vertices, faces and error texts are then the reference's for the same bytes.
 //
-// Deliberate differences, where the reference's behaviour is undefined or a
-// crash: a NaN coordinate never merges in weld (the reference orders vertices
-// with operator<, which NaN breaks); element counts in headers reserve no
-// memory up front, so a corrupt count cannot abort the process.
+// Deliberate differences, where the reference's behaviour is undefined, a
+// crash or a near-endless loop: a NaN coordinate never merges in weld (the
+// reference orders vertices with operator<, which NaN breaks); element counts
+// in headers reserve no memory up front, so a corrupt count cannot abort the
+// process; a binary PLY element without properties is skipped instead of
+// walking its claimed item count (its items occupy no bytes).
 #include "../../include/del3d_b200.h"
 #include "../../include/del3d/mesh_io.h"
 
