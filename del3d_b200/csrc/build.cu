@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <mutex>
 #include <numeric>
+#include <optional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1650,6 +1651,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         }
     } ph_guard{ph};
     cudaEventRecord(ph[0], s);
+    NvtxRange nvtx_build("d3g.build");
+    std::optional<NvtxRange> nvtx_phase;
+    nvtx_phase.emplace("d3g.order");
     // ---- insertion order and duplicate groups ----
     DevBuf<int32_t> order;
     D3G_TRY(order.alloc(size_t(N), s));
@@ -1715,6 +1719,8 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     for (int i = 0; i < nsets; ++i) R.set_nv[size_t(i)] = hvoff[size_t(i) + 1] - hvoff[size_t(i)];
 
     cudaEventRecord(ph[1], s);
+    nvtx_phase.reset();
+    nvtx_phase.emplace("d3g.insert");
     // ---- each set's first tet: its first four affinely independent vertices ----
     DevBuf<int> found;
     DevBuf<int4> skips;
@@ -2033,6 +2039,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         const double alpha_eff = level_alpha(lev);
         W.n = level_descs(lev, alpha_eff, descs);
         if (W.n == 0) continue;
+        char level_name[32];
+        std::snprintf(level_name, sizeof level_name, "d3g.level %d", lev);
+        NvtxRange nvtx_level(level_name);
         std::fill(hp0.begin(), hp0.end(), 0);
         std::fill(hw.begin(), hw.end(), 0);
         for (size_t i = 0; i < descs.size(); ++i) {
@@ -2253,6 +2262,8 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     fnew.release();
 
     cudaEventRecord(ph[2], s);
+    nvtx_phase.reset();
+    nvtx_phase.emplace("d3g.output");
     // ---- output: canonical cells ----
     int ntet = 0;
     D3G_CUDA(cudaMemcpyAsync(&ntet, tet_count.p, sizeof ntet, cudaMemcpyDeviceToHost, s));

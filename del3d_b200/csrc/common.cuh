@@ -6,6 +6,7 @@
 #include "predicates.cuh"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -94,6 +95,18 @@ struct DevBuf {
         std::swap(cap, o.cap);
         std::swap(dev, o.dev);
     }
+};
+
+/// A named NVTX range over a scope: a host-side marker that costs nothing
+/// without a profiler attached.  The build marks d3g.build, d3g.order,
+/// d3g.insert, "d3g.level N" and d3g.output, and the server each batch
+/// (d3g.server.batch), so a profiler can pick the kernels of one phase
+/// (ncu --nvtx --nvtx-include).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 inline unsigned grid_for(int64_t n, int block, int64_t cap = int64_t(kNumSMs) * 32) {

@@ -103,6 +103,7 @@ void copy_error(Request* r, int status) {
 /// Builds `batch` on `stream` and fills each request's result.  Returns the
 /// status of the batch build (per-request statuses are set either way).
 int run_batch(const std::vector<Request*>& batch, cudaStream_t stream) {
+    NvtxRange nvtx_batch("d3g.server.batch");
     const int k = int(batch.size());
     std::vector<int64_t> off(size_t(k) + 1, 0);
     for (int i = 0; i < k; ++i) off[size_t(i) + 1] = off[size_t(i)] + batch[size_t(i)]->n;
