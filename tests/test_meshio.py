@@ -267,3 +267,25 @@ def test_bench_readers_workload_line():
     assert line["unit"] == "points/s" and line["value"] > 0 and line["sets_equal_input"]
     if oracle.ref_meshio_available():
         assert line["equals_reference"] and line["cpu_baseline"]["kind"] == "reference"
+
+
+def test_c_abi_argument_errors():
+    lib = d3.library()
+    m = d3._Mesh()
+    assert lib.d3g_mesh_load(None, ctypes.byref(m)) == 1
+    assert lib.d3g_read_xyz(b"x.xyz", None) == 1
+    assert lib.d3g_mesh_weld(None) == 1
+    bad = d3._Mesh(None, None, 3, 0)                       # vertices missing
+    assert lib.d3g_mesh_weld(ctypes.byref(bad)) == 1
+    assert lib.d3g_mesh_drop_non_finite(ctypes.byref(bad), None) == 1
+    v = np.zeros((2, 3))
+    f = np.array([[0, 1, 5]], np.int32)                   # face index out of range
+    mm = d3._Mesh(v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), f.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                  2, 1)
+    assert lib.d3g_mesh_weld(ctypes.byref(mm)) == 2
+    assert lib.d3g_mesh_drop_non_finite(ctypes.byref(mm), None) == 2
+    ps = d3._PointSets()
+    assert lib.d3g_load_point_sets(None, 2, 1, ctypes.byref(ps)) == 1
+    assert lib.d3g_load_point_sets(None, 0, 1, None) == 1
+    lib.d3g_mesh_free(None)
+    lib.d3g_point_sets_free(None)

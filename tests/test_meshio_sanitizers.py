@@ -41,3 +41,25 @@ def test_readers_clean_under_address_and_ub_sanitizers(tmp_path):
         assert r.returncode == 0 and r.stdout.startswith("ok"), r.stderr[-3000:]
     r = subprocess.run([exe, big_path, big_path], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stderr[-3000:]
+
+
+def test_threaded_loading_clean_under_thread_sanitizer(tmp_path):
+    """d3g_load_point_sets on worker threads, and a large text file cut into
+    pieces parsed on more threads inside them."""
+    import numpy as np
+
+    exe = _build(tmp_path, ["-fsanitize=thread"])
+    rng = np.random.default_rng(8)
+    chunk = b"".join(mc.random_xyz(rng) for _ in range(1500))
+    big = []
+    for k in range(3):
+        p = str(tmp_path / f"big{k}.xyz")
+        with open(p, "wb") as fh:
+            while fh.tell() < (5 << 20):
+                fh.write(chunk)
+        big.append(p)
+    small = mc.write_cases(str(tmp_path / "hand"), {k: v for k, v in mc.hand_cases().items() if not v.startswith(b"solid")})
+    env = dict(os.environ, TSAN_OPTIONS="halt_on_error=1")
+    r = subprocess.run([exe] + big + small, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0 and r.stdout.startswith("ok") and "WARNING: ThreadSanitizer" not in r.stderr, \
+        r.stderr[-3000:]
