@@ -36,7 +36,7 @@ __all__ = [
     "collinear", "spatial_sort", "library", "LIB_PATH", "predicate_stats", "circumcenters",
     "circumcenter", "circumcenter_lazy", "Server", "Request", "pool_usage",
     "release_cached_memory", "load_mesh", "read_xyz", "weld", "drop_non_finite",
-    "supported_formats", "load_point_sets", "partition_sets",
+    "supported_formats", "load_point_sets", "partition_sets", "validate_cells",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -222,6 +222,8 @@ def library() -> ctypes.CDLL:
     lib.d3g_load_point_sets.restype = _INT
     lib.d3g_point_sets_free.argtypes = [ctypes.POINTER(_PointSets)]
     lib.d3g_point_sets_free.restype = None
+    lib.d3g_validate_cells.argtypes = [_P, _I64, _I64]
+    lib.d3g_validate_cells.restype = _INT
     for name in ("d3g_predicates", "d3g_predicates_device", "d3g_orient2d", "d3g_spatial_sort",
                  "d3g_spatial_sort_device", "d3g_shuffle_device", "d3g_build", "d3g_build_device"):
         getattr(lib, name).restype = _INT
@@ -885,3 +887,16 @@ def load_point_sets(paths, threads: int = 0):
         return xyz, offs, dropped
     finally:
         lib.d3g_point_sets_free(ctypes.byref(ps))
+
+
+# ---- checking a result (host) ---------------------------------------------------------
+
+
+def validate_cells(all_cells, n_points: int = 0) -> None:
+    """Checks all_cells() (infinite vertex -1) as the reference's Tds::validate()
+    checks its cell table: distinct vertices in range, every facet shared by two
+    consistently oriented cells, Euler characteristic 0.  Raises Del3dError with
+    the first violation.  Host only."""
+    t = np.ascontiguousarray(all_cells, dtype=np.int32).reshape(-1, 4)
+    _check(library().d3g_validate_cells(_ptr(t) if t.shape[0] else None, t.shape[0], int(n_points)),
+           "validate_cells")

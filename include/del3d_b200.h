@@ -346,6 +346,17 @@ int d3g_reset_tuning(void);
  * independent chains per thread.  No counterpart in the reference. */
 int d3g_microbench_fp64(int64_t iters, double* addmul_ops_per_s, double* fma_per_s, void* stream);
 
+/* ---- checking a result (host) ---------------------------------------------------
+ * The output-side counterpart of the reference's Tds::validate() (src/tds.h:483-530)
+ * for all_cells() (infinite vertex = -1; any cell order, any even rotation): every
+ * cell has four distinct vertices in [-1, n_points) (n_points <= 0: no upper bound)
+ * with at most one infinite; every triangular facet is shared by exactly two cells
+ * inducing opposite orientations on it; the Euler characteristic V - E + F - T is 0
+ * (a triangulated 3-sphere: the hull closed through the infinite vertex).  Returns
+ * D3G_OK, or D3G_ERR_INVALID_INPUT with the first violation in d3g_last_error().
+ * No device is needed. */
+int d3g_validate_cells(const int32_t* all_cells, int64_t n_cells, int64_t n_points);
+
 /* ---- input readers (host) -------------------------------------------------------
  * The point and mesh formats of the reference's viewer reader (replaces
  * meshio::load / weld / drop_non_finite / supported_formats,
