@@ -86,9 +86,12 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "plain", "predicates", "sort", "readers"],
+                    choices=["batched", "plain", "c3", "predicates", "sort", "readers"],
                     help="batched: the headline line; plain: one single-set build per step "
-                         "(--n uniform points); predicates / sort: the predicate and "
+                         "(--n uniform points); c3: the four plain single-set configurations "
+                         "(1e6 uniform, the 100^3 lattice, 1e6 quantised sphere, 1e7 uniform), "
+                         "each timed and compared with the reference's build; predicates / sort: "
+                         "the predicate and "
                          "spatial-sort microbenchmarks, one line each; readers: the host "
                          "input readers on files of a sample of the batched sets (no GPU)")
     ap.add_argument("--n", type=int, default=PLAIN_N, help="points of the plain workload")
@@ -139,10 +142,14 @@ def measured_peaks():
         return {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
 
 
-def workload_sets(n_sets, rank):
-    import del3d_b200 as d3
+def workload_sets(n_sets, rank, gen=None):
+    """The sets of rank `rank`.  `gen` is the module whose generators make them:
+    del3d_b200 for our arm, the oracle's copy of the same generators for the
+    reference arm (which must not load the product library)."""
+    if gen is None:
+        import del3d_b200 as gen
 
-    return d3.mixed_workload(n_sets, LO, HI, seed=2024 + rank, first_seed=1000 + n_sets * rank)
+    return gen.mixed_workload(n_sets, LO, HI, seed=2024 + rank, first_seed=1000 + n_sets * rank)
 
 
 def rank_sets(n_sets, rank, world, scaling):
@@ -330,7 +337,7 @@ def run_reference(args):
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
         return 0
-    sets = workload_sets(args.sets, 0)
+    sets = workload_sets(args.sets, 0, gen=oracle)
     sample = cpu_sample(sets)
     threads = host_threads()
     times, pts = [], 0
@@ -806,6 +813,7 @@ def run_predicates(args):
     pts = torch.from_numpy(pts_h).to(dev)
     lib = d3.library()
     res = {}
+    parity_ok = True
     for kind, name, k, base, groups, ops in ((d3.ORIENT3D, "orient3d", 4, pbase, g4, ORIENT3D_OPS),
                                              (d3.IN_SPHERE, "in_sphere", 5, sbase, g5, IN_SPHERE_OPS)):
         idx = predicate_queries(torch, dev, k, n_uni, base, groups, PRED_QUERIES, 7 + k)
@@ -834,6 +842,27 @@ def run_predicates(args):
                      "fp64_ops_per_query": ops, "fp64_ops_per_s": qps * ops,
                      "fp64_frac_of_measured_addmul_peak": qps * ops / addmul,
                      "signs_neg_zero_pos": signs}
+        if not args.no_cpu_baseline:
+            # Sign parity, after the timed calls: a strided sample of the timed
+            # stream, plus one query on every degenerate group, against the
+            # reference's predicate and the reference's integer oracle.
+            sample_idx = idx[::PRED_SAMPLE_STRIDE].cpu().numpy()
+            sample_got = out[::PRED_SAMPLE_STRIDE].cpu().numpy()
+            grp = np.arange(groups, dtype=np.int64)
+            rot = grp % k
+            gidx = (base + grp[:, None] * k + (np.arange(k)[None, :] + rot[:, None]) % k).astype(np.int32)
+            gidx_d = torch.from_numpy(gidx).to(dev)
+            gout = torch.empty(groups, dtype=torch.int8, device=dev)
+            d3._check(lib.d3g_predicates_device(pts.data_ptr(), pts.shape[0], gidx_d.data_ptr(), groups, kind,
+                                                gout.data_ptr(), ctypes.c_void_p(stream.cuda_stream),
+                                                ctypes.byref(st)), name)
+            torch.cuda.synchronize()
+            res[name]["parity"] = predicate_parity(pts_h, name, [(sample_idx, sample_got),
+                                                                  (gidx, gout.cpu().numpy())])
+            res[name]["parity"]["sample"] = (f"every {PRED_SAMPLE_STRIDE}th query of the timed stream "
+                                             f"({sample_idx.shape[0]}) plus one query per degenerate group "
+                                             f"({groups}, point order rotated)")
+            parity_ok = parity_ok and res[name]["parity"]["equal"]
         del idx, out
     line = {"metric": "predicate queries/s (filter + exact stage + perturbation)",
             "value": 2 * PRED_QUERIES / sum(r["ms"] / 1000.0 for r in res.values()),
@@ -847,8 +876,40 @@ def run_predicates(args):
             "fp64_peak": {"addmul_ops_per_s": addmul, "dfma_per_s": fma,
                           "note": "measured here by d3g_microbench_fp64"},
             "predicates": res}
+    if not args.no_cpu_baseline:
+        line["parity"] = parity_ok
     print(json.dumps(line))
-    return 0
+    return 0 if parity_ok else 1
+
+
+PRED_SAMPLE_STRIDE = 100
+
+
+def predicate_parity(pts, name, batches):
+    """Signs the GPU gave (`batches`: (index tuples, signs) pairs) against the
+    reference's predicate (oracle/_ref) and its integer oracle tests/exact.h,
+    evaluated on host threads.  None when the reference is absent."""
+    import numpy as np
+
+    import oracle
+
+    if not oracle.ref_available():
+        return {"equal": True, "checked": 0, "note": "reference not built: not checked"}
+    kind = "in_sphere" if name == "in_sphere" else "orient3d"
+    idx = np.concatenate([b[0] for b in batches])
+    got = np.concatenate([b[1] for b in batches])
+    pieces = np.array_split(np.arange(idx.shape[0]), host_threads() * 4)
+
+    def one(fn, part):
+        return fn(kind, pts, idx[part])
+
+    with ThreadPoolExecutor(max_workers=host_threads()) as ex:
+        ref = np.concatenate(list(ex.map(lambda pt: one(oracle.ref_predicate, pt), pieces)))
+        exact = np.concatenate(list(ex.map(lambda pt: one(oracle.exact_predicate, pt), pieces)))
+    return {"equal": bool(np.array_equal(got, ref) and np.array_equal(got, exact)), "checked": int(idx.shape[0]),
+            "differ_from_reference": int(np.count_nonzero(got != ref)),
+            "differ_from_exact": int(np.count_nonzero(got != exact)),
+            "zero_signs": int(np.count_nonzero(got == 0))}
 
 
 def run_plain(args):
@@ -885,6 +946,85 @@ def run_plain(args):
                       "build_stats": {k: (round(v, 3) if isinstance(v, float) else v)
                                       for k, v in stats.items()}}))
     return 0
+
+
+# The plain single-set configurations: (name, distribution, points, seed).
+C3_CONFIGS = (("uniform_1e6", "uniform", 1_000_000, 4),
+              ("lattice_100^3", "lattice", 1_000_000, 0),
+              ("sphere_1e6_q1024_dedup", "sphere", 1_000_000, 5),
+              ("uniform_1e7", "uniform", 10_000_000, 6))
+
+
+def run_c3(args):
+    """The four plain single-set configurations: each built on the GPU through
+    d3g_build_device (device-resident input, CUDA events, --warmup untimed then
+    --steps timed builds), then its cells compared with the reference's build of
+    the same points (oracle/_ref, canonical order).  The reference builds run on
+    host threads while the GPU works; each is single-threaded, and its time is
+    reported beside the GPU's.  Exits 1 if any set of cells differs."""
+    import numpy as np
+    import torch
+
+    import del3d_b200 as d3
+    import oracle
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    inputs = [(name, d3.gen_set(dist, n, seed)) for name, dist, n, seed in C3_CONFIGS]
+    check = oracle.ref_available() and not args.no_cpu_baseline
+
+    def ref_one(pts):
+        t0 = time.perf_counter()
+        r = oracle.ref_build(pts)
+        t = time.perf_counter() - t0
+        return oracle.canonical_cells(r["cells"]), int(r["n_vertices"]), t
+
+    pool = ThreadPoolExecutor(max_workers=len(inputs)) if check else None
+    futures = [pool.submit(ref_one, pts) for _, pts in inputs] if check else None
+    rows, all_equal = [], True
+    for k, (name, pts) in enumerate(inputs):
+        x = torch.from_numpy(pts).to(dev)
+        n = x.shape[0]
+        out = torch.empty((8 * n + 64, 4), dtype=torch.int32, device=dev)
+        ms = []
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                d3.build_device(x, out=out, stream=stream.cuda_stream)
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                cells, nv = d3.build_device(x, out=out, stream=stream.cuda_stream)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        got = cells.cpu().numpy()
+        row = {"config": name, "points": int(n), "ms_median": statistics.median(ms), "ms_min": min(ms),
+               "points_per_s": n / (statistics.median(ms) / 1000.0), "tets": int(got.shape[0]),
+               "n_vertices": int(nv)}
+        if check:
+            want, ref_nv, t_ref = futures[k].result()
+            equal = bool(got.shape == want.shape and np.array_equal(got, want) and ref_nv == nv)
+            all_equal = all_equal and equal
+            row.update({"reference_tets": int(want.shape[0]), "parity": equal,
+                        "reference_s_1thread": t_ref, "gpu_over_reference": t_ref / (row["ms_median"] / 1000.0)})
+        rows.append(row)
+        del x, out, cells
+        torch.cuda.empty_cache()
+    if pool:
+        pool.shutdown()
+    line = {"metric": "plain single-set build points/s at bit-exact tet sets", "unit": "points/s",
+            "value": rows[-1]["points_per_s"], "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "plain single-set builds: 1e6 uniform [0,1)^3 (seed 4), the 100^3 integer "
+                                   "lattice, 1e6 unit-sphere samples quantised to 2^-10 with duplicates removed "
+                                   "(seed 5), 1e7 uniform (seed 6); value = the 1e7 build",
+                       "reference": "oracle/_ref (the reference compiled from source), one thread per build, "
+                                    "the four running concurrently on host threads while the GPU builds"},
+            "builds": rows, "parity": (all_equal if check else None)}
+    print(json.dumps(line))
+    return 0 if all_equal else 1
 
 
 SORT_N = 10_000_000
@@ -1036,6 +1176,8 @@ def main():
         return run_sort(args)
     if args.workload == "plain":
         return run_plain(args)
+    if args.workload == "c3":
+        return run_c3(args)
     return run_ours(args)
 
 

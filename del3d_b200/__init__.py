@@ -48,6 +48,21 @@ _I32 = ctypes.c_int32
 _INT = ctypes.c_int
 
 
+# d3g_status values (include/del3d_b200.h).
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_INVALID_INPUT = 2
+ERR_OOM = 3
+ERR_EXACT_CAPACITY = 4
+ERR_CAVITY_CAPACITY = 5
+ERR_WALK_LIMIT = 6
+ERR_ROUND_LIMIT = 7
+ERR_CUDA = 8
+ERR_INTERNAL = 9
+ERR_NO_DEVICE = 10
+ERR_NOT_READY = 11
+
+
 class Del3dError(RuntimeError):
     """A non-OK status from the C ABI (the reference has no error channel; this
     library never fails silently)."""
@@ -86,7 +101,8 @@ class _Result(ctypes.Structure):
 class _Options(ctypes.Structure):
     _fields_ = [("want_all_cells", _I32), ("want_incident", _I32), ("chunk", _I32),
                 ("max_rounds", _I32), ("timing", _I32), ("alpha_small", _I32), ("split", _I32),
-                ("lanes", _I32), ("schedule", _I32)]
+                ("lanes", _I32), ("schedule", _I32), ("tet_capacity", _I32), ("walk_limit", _I32),
+                ("cavity_capacity", _I32)]
 
 
 class _BatchResult(ctypes.Structure):
@@ -479,11 +495,15 @@ def _apply(opts, **kw):
 
 def build_device(points_dev, out=None, stream: int = 0, chunk: Optional[int] = None, timing: bool = False,
                  stats: Optional[dict] = None, alpha_small: Optional[int] = None, split: Optional[int] = None,
-                 lanes: Optional[int] = None, schedule: Optional[int] = None):
+                 lanes: Optional[int] = None, schedule: Optional[int] = None, max_rounds: Optional[int] = None,
+                 tet_capacity: Optional[int] = None, walk_limit: Optional[int] = None,
+                 cavity_capacity: Optional[int] = None):
     """Builds from a device-resident torch tensor (n, 3) float64 on `stream`
     (a raw cudaStream_t handle; 0 = default) and returns the canonical finite
     cells as a device int32 tensor view (n_cells, 4) and the vertex count.
-    `out` may supply the (cap, 4) int32 output buffer.  Synchronises `stream`."""
+    `out` may supply the (cap, 4) int32 output buffer.  Synchronises `stream`.
+    max_rounds / tet_capacity / walk_limit / cavity_capacity lower the build's
+    limits (d3g_options), which makes their failure statuses reachable."""
     import torch
 
     lib = library()
@@ -496,7 +516,8 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: Optional[int] = N
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
     _apply(opts, chunk=chunk, timing=int(timing), alpha_small=alpha_small, split=split, lanes=lanes,
-           schedule=schedule)
+           schedule=schedule, max_rounds=max_rounds, tet_capacity=tet_capacity, walk_limit=walk_limit,
+           cavity_capacity=cavity_capacity)
     st = BuildStats()
     _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), out.shape[0],
                                 ctypes.byref(nc), ctypes.byref(nv), _P(stream), ctypes.byref(st)),

@@ -58,8 +58,8 @@ constexpr int kRotateLimit = 1 << 16;
 constexpr int kRoundsPerBatch = 16;
 // Scratch of a worker in a normal round, and of each of the kBigSlots workers
 // served at a time in a big round.
-constexpr int kCavCap = 256, kFacCap = 512;
-constexpr int kBigSlots = 64, kBigCav = 16384, kBigFac = 32768;
+constexpr int kCavCap = 256;                     // boundary facets: twice the tets
+constexpr int kBigSlots = 64, kBigCav = 16384;   // boundary facets: twice the tets
 
 enum : int { WS_DONE = 0, WS_CAND = 1, WS_LOST = 2, WS_WIN = 3, WS_PARKED = 4, WS_FAIL = 5 };
 
@@ -93,6 +93,7 @@ struct Tables {
     int* vert_tet;             // one live tet incident to each inserted vertex
     int* tet_count;
     int cap;
+    int walk_limit;            // steps of a lockstep walk before ST_WALK_LIMIT
 };
 
 struct Workers {
@@ -315,7 +316,7 @@ __device__ int walk_g(bool live, int t, const Pt& p, int pid, const Tables& T, c
                     prev = t;
                     t = next;
                     tv = nv;
-                    if (step + 1 >= kWalkLimit) {
+                    if (step + 1 >= T.walk_limit) {
                         report(st, ST_WALK_LIMIT);
                         walking = false;
                     }
@@ -674,7 +675,7 @@ __device__ __forceinline__ int4 ld4(const int4* p) { return __ldcg(p); }
 
 /// Visibility walk on a mesh other warps are changing: reads go to L2 and may
 /// be stale, so the tet it returns is only a candidate, checked under its lock.
-/// Returns -1 after kAsyncWalkLimit steps.
+/// Returns -1 after kAsyncWalkLimit steps (or the build's walk limit, if lower).
 __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
                           bool ex, uint32_t* st, int lane) {
     int4 tv = ld4(T.tv + t);
@@ -687,7 +688,8 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
     }
     int prev = -1;
     uint32_t h = uint32_t(pid) * 2654435761u + 12345u;
-    for (int step = 0; step < kAsyncWalkLimit; ++step) {
+    const int limit = min(kAsyncWalkLimit, T.walk_limit);
+    for (int step = 0; step < limit; ++step) {
         const int4 tn = ld4(T.tn + t);
         h = h * 1664525u + 1013904223u;
         const int s0 = int(h >> 30);
@@ -1753,9 +1755,11 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
 
     // ---- tables ----
     Tables T;
-    int64_t cap64 = int64_t(nv) * 8 + 5 * int64_t(nsets) + 4096;
+    const int tets_per_vertex = opt.tet_capacity > 0 ? opt.tet_capacity : 8;
+    int64_t cap64 = int64_t(nv) * tets_per_vertex + 5 * int64_t(nsets) + 4096;
     if (cap64 > (int64_t(1) << 29)) cap64 = int64_t(1) << 29;
     T.cap = int(cap64);
+    T.walk_limit = opt.walk_limit > 0 ? opt.walk_limit : kWalkLimit;
     DevBuf<int4> tv, tn;
     DevBuf<unsigned long long> claim;
     DevBuf<uint8_t> alive;
@@ -1875,8 +1879,12 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     const bool grow = opt.chunk <= 0 && opt.split != 0;
     if (grow) maxw = std::max<int>(maxw, int(std::min<int64_t>(int64_t(nv) / 16, int64_t(1) << 18)));
     Workers W;
-    W.cav_cap = kCavCap;
-    W.fac_cap = kFacCap;
+    // Conflict-region scratch per worker (normal rounds and asynchronous
+    // passes) and per big-round slot; a caller's cavity_capacity lowers both.
+    const int cav_normal = opt.cavity_capacity > 0 ? std::min(kCavCap, int(opt.cavity_capacity)) : kCavCap;
+    const int cav_big = opt.cavity_capacity > 0 ? std::min(kBigCav, int(opt.cavity_capacity)) : kBigCav;
+    W.cav_cap = cav_normal;
+    W.fac_cap = 2 * cav_normal;
     W.n = maxw;
     DevBuf<int> wcur, wbeg, wend, wpos, wleft, wnwon, wlast, wguide, wstate, wncav, wnfac, wcav, wfac, counters;
     DevBuf<int> set_p0, set_ins, set_w, set_split, nworkers;
@@ -1981,10 +1989,10 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         if (!blist.p) {
             D3G_TRY(blist.alloc(size_t(maxw), s));
             D3G_TRY(bcount.alloc(1, s));
-            D3G_TRY(bcav.alloc(size_t(kBigSlots) * kBigCav, s));
-            D3G_TRY(bfac.alloc(size_t(kBigSlots) * kBigFac, s));
-            D3G_TRY(bsv.alloc(size_t(kBigSlots) * kBigFac, s));
-            D3G_TRY(bsn.alloc(size_t(kBigSlots) * kBigFac, s));
+            D3G_TRY(bcav.alloc(size_t(kBigSlots) * cav_big, s));
+            D3G_TRY(bfac.alloc(size_t(kBigSlots) * 2 * cav_big, s));
+            D3G_TRY(bsv.alloc(size_t(kBigSlots) * 2 * cav_big, s));
+            D3G_TRY(bsn.alloc(size_t(kBigSlots) * 2 * cav_big, s));
         }
         for (;;) {
             D3G_CUDA(cudaMemsetAsync(bcount.p, 0, sizeof(int), s));
@@ -2000,8 +2008,8 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             WB.fac = bfac.p;
             WB.st_v = bsv.p;
             WB.st_n = bsn.p;
-            WB.cav_cap = kBigCav;
-            WB.fac_cap = kBigFac;
+            WB.cav_cap = cav_big;
+            WB.fac_cap = 2 * cav_big;
             for (;;) {
                 if (++round > max_rounds) {
                     set_error("d3g_build: insertion round limit reached");
@@ -2390,6 +2398,9 @@ void d3g_options_default(d3g_options* o) {
     o->lanes = 0;
     o->schedule = 0;
     o->split = 0;
+    o->tet_capacity = 0;
+    o->walk_limit = 0;
+    o->cavity_capacity = 0;
     d3g_tuning t;
     if (current_tuning(&t)) {
         o->schedule = t.schedule;

@@ -12,6 +12,8 @@
 // kernel per query.
 #include "common.cuh"
 
+#include <cuda.h>
+
 #include <mutex>
 
 namespace d3g {
@@ -270,12 +272,44 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
+/// Identity of the calling thread's current CUDA context (driver entry points
+/// reached through the runtime, so no link to the driver library is needed);
+/// false if it cannot be had.
+bool current_context_id(unsigned long long* id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
 /// The device address of g_noalloc_scratch on the current device.  In host
 /// code the symbol is a host-side stand-in, not a device address, so it is
-/// looked up once per device (with that device current) and cached.
+/// looked up with the device current (cudaGetSymbolAddress) on the first call
+/// in each context of a device and cached.  The cache is keyed on the context's
+/// identity as well as the device ordinal: after a cudaDeviceReset the module
+/// is loaded again into a new context, where the array may sit elsewhere, and
+/// the first call there looks it up anew.  Without a context identity (no
+/// driver entry point) the address is looked up on every call.
 int noalloc_scratch(NoAllocScratch** out) {
     static std::mutex mu;
     static NoAllocScratch* addr[64] = {};
+    static unsigned long long ctx_of[64] = {};
     int dev = 0;
     const cudaError_t ge = cudaGetDevice(&dev);
     if (ge != cudaSuccess || dev < 0 || dev >= 64) {
@@ -283,8 +317,10 @@ int noalloc_scratch(NoAllocScratch** out) {
         set_error("d3g_predicates_noalloc_device: no usable current device");
         return D3G_ERR_NO_DEVICE;
     }
+    unsigned long long ctx = 0;
+    bool have_ctx = current_context_id(&ctx);
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (!addr[dev] || !have_ctx || ctx_of[dev] != ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -292,7 +328,11 @@ int noalloc_scratch(NoAllocScratch** out) {
             set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             return D3G_ERR_CUDA;
         }
+        // The lookup makes the device's primary context current if none was:
+        // record the identity of the context the address belongs to.
+        if (!have_ctx) have_ctx = current_context_id(&ctx);
         addr[dev] = static_cast<NoAllocScratch*>(p);
+        ctx_of[dev] = have_ctx ? ctx : 0;
     }
     *out = addr[dev];
     return D3G_OK;

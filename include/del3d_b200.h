@@ -108,7 +108,9 @@ int d3g_predicates_device(const double* d_pts, int64_t n_pts, const int32_t* d_i
  *   - At most D3G_NOALLOC_MAX_QUERIES queries per call; more returns
  *     D3G_ERR_INVALID_ARGUMENT without touching the device.
  *   - The first call on a device looks up the array's device address; make that
- *     first call before any stream capture.
+ *     first call before any stream capture.  A cudaDeviceReset gives the device a
+ *     new context, where the first call looks the address up again (and so
+ *     should come before any capture there too).
  *   - Every call reuses the same array (the counters are cleared per call):
  *     calls that overlap on the GPU, on any streams, race with each other.
  * Synchronises `stream`. */
@@ -167,6 +169,19 @@ typedef struct d3g_options {
                              /* kernels: 32, 16, 8 or 4; 0 = 32 (default)        */
     int32_t schedule;        /* 0 = asynchronous insertion with rounds for what  */
                              /* it leaves (default); 1 = lockstep rounds only    */
+    /* Capacities and step limits (0 = the built-in value).  Lowering one makes
+     * its failure path reachable on small input, for testing: the build then
+     * stops with the status named, returns no cells, and the device stays
+     * usable for the next call. */
+    int32_t tet_capacity;    /* tet-table slots per vertex (built-in 8);         */
+                             /* too few: D3G_ERR_OOM ("tet table full")          */
+    int32_t walk_limit;      /* steps of a point-location walk (built-in 2^20    */
+                             /* in the rounds, 2^14 per asynchronous attempt);   */
+                             /* exceeded: D3G_ERR_WALK_LIMIT                     */
+    int32_t cavity_capacity; /* conflict-region tets a worker may hold: caps the */
+                             /* normal scratch (256) and the big-round scratch   */
+                             /* (16384), boundary facets at twice it; exceeded   */
+                             /* in a big round: D3G_ERR_CAVITY_CAPACITY          */
 } d3g_options;
 
 /* What a build did (filled by d3g_build and d3g_build_device). */

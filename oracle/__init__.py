@@ -65,6 +65,12 @@ def orc() -> ctypes.CDLL:
         lib.orc_build_all.argtypes = [_P, _P]
         lib.orc_build_free.argtypes = [_P]
         lib.orc_canonical_rotate.argtypes = [_P, _I64]
+        lib.d3g_gen_uniform.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, _P]
+        lib.d3g_gen_sphere.argtypes = [_I64, ctypes.c_uint32, ctypes.c_double, ctypes.c_int32, _P]
+        lib.d3g_gen_clusters.argtypes = [_I64, ctypes.c_uint32, ctypes.c_int32, ctypes.c_double, _P]
+        lib.d3g_gen_lattice.argtypes = [_I64, _P]
+        for name in ("d3g_gen_uniform", "d3g_gen_sphere", "d3g_gen_clusters", "d3g_gen_lattice"):
+            getattr(lib, name).restype = None
         _orc = lib
     return _orc
 
@@ -305,6 +311,48 @@ def ps_rng_below(seed: int, m: int, count: int) -> np.ndarray:
     out = np.zeros(count, dtype=np.int64)
     ref().ps_rng_below(seed, m, count, _ptr(out))
     return out
+
+
+# ---- the benchmarks' synthetic point sets, without the product library ------------
+#
+# The same generators as del3d_b200.gen_set / mixed_workload (liboracle.so is
+# compiled with del3d_b200/csrc/pointgen.cpp), so that the reference's timed arm
+# of bench.py builds exactly the GPU arm's inputs without loading
+# libdel3d_b200.so.  tests/test_oracle.py checks the two agree bit for bit.
+
+DISTRIBUTIONS = ("uniform", "clusters", "lattice", "sphere")
+
+
+def gen_set(dist: str, n: int, seed: int) -> np.ndarray:
+    lib = orc()
+    out = np.zeros((n, 3), dtype=np.float64)
+    if n == 0:
+        return out
+    if dist == "uniform":
+        lib.d3g_gen_uniform(n, seed, 0.0, 1.0, _ptr(out))
+    elif dist == "clusters":
+        lib.d3g_gen_clusters(n, seed, 8, 0.02, _ptr(out))
+    elif dist == "lattice":
+        lib.d3g_gen_lattice(n, _ptr(out))
+    else:
+        lib.d3g_gen_sphere(n, seed, 1.0, 1024, _ptr(out))
+        _, first = np.unique(out, axis=0, return_index=True)
+        out = out[np.sort(first)]
+    return out
+
+
+def gen_uniform(n: int, seed: int, lo: float = 0.0, hi: float = 1.0) -> np.ndarray:
+    out = np.zeros((n, 3), dtype=np.float64)
+    if n:
+        orc().d3g_gen_uniform(n, seed, lo, hi, _ptr(out))
+    return out
+
+
+def mixed_workload(n_sets: int, lo: int = 32, hi: int = 65536, seed: int = 2024, first_seed: int = 1000):
+    rng = np.random.default_rng(seed)
+    sizes = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), n_sets))).astype(np.int64)
+    dists = rng.integers(0, len(DISTRIBUTIONS), n_sets)
+    return [gen_set(DISTRIBUTIONS[d], int(n), first_seed + k) for k, (n, d) in enumerate(zip(sizes, dists))]
 
 
 # ---- the reference viewer's mesh reader ------------------------------------------------

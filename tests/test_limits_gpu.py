@@ -1,0 +1,99 @@
+"""Failure paths of the build, forced from the host by lowering a limit
+(d3g_options): each must end the call with its status - never a hang, a trap
+or corrupt cells - and the next build on the same device must still equal the
+reference.  Every limit here is a bounded loop or a capacity check on the
+device that records a status word the host reads; nothing faults the GPU.
+The reference has no error channel (it grows without bound and aborts only
+under DEL3D_VALIDATE, src/triangulation.cpp:110-118); its walk budget is
+src/triangulation.cpp:368-369."""
+import numpy as np
+import pytest
+
+import del3d_b200 as d3
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _expect(status, pts, **limits):
+    import torch
+
+    x = torch.from_numpy(pts).to("cuda")
+    with pytest.raises(d3.Del3dError) as e:
+        d3.build_device(x, **limits)
+    assert e.value.status == status, (e.value, limits)
+
+
+def _still_correct():
+    """A normal build right after the failure equals the reference."""
+    pts = d3.gen_lattice(20 ** 3)
+    d = d3.Delaunay()
+    d.build(pts)
+    want = oracle.canonical_cells(oracle.ref_build(pts)["cells"])
+    assert np.array_equal(d.finite_cells(), want)
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_round_limit(cuda, schedule):
+    # Lockstep rounds go out 16 to a batch: a limit of 1 is hit by the first batch
+    # (schedule 1), or by the first batch the asynchronous pass's leftovers need.
+    pts = d3.gen_lattice(20_000)
+    if schedule == 0:
+        _expect(d3.ERR_ROUND_LIMIT, pts, schedule=0, max_rounds=1, walk_limit=1)
+    else:
+        _expect(d3.ERR_ROUND_LIMIT, pts, schedule=1, max_rounds=1)
+    _still_correct()
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_tet_capacity(cuda, schedule):
+    # One tet slot per vertex where uniform input needs about 6.75: the table
+    # fills and the build reports it instead of writing past it.
+    _expect(d3.ERR_OOM, d3.gen_uniform(20_000, 3), schedule=schedule, tet_capacity=1)
+    _still_correct()
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_walk_limit(cuda, schedule):
+    # One step per walk: the asynchronous attempts give up and leave their points
+    # to the rounds, whose walks then stop at the limit with a status.
+    _expect(d3.ERR_WALK_LIMIT, d3.gen_uniform(20_000, 3), schedule=schedule, walk_limit=1)
+    _still_correct()
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_cavity_capacity(cuda, schedule):
+    # Two region tets per worker, in the normal and the big-round scratch alike:
+    # a region that outgrows the big-round scratch reports its status.
+    _expect(d3.ERR_CAVITY_CAPACITY, d3.gen_uniform(20_000, 3), schedule=schedule, cavity_capacity=2)
+    _still_correct()
+
+
+def _wide_octahedron(k):
+    """The unit octahedron's vertices with one moved off the sphere by 2^-k in
+    x: in_sphere calls on it are uncertain for the filter, and their exact
+    values span about k binades."""
+    pts = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [-1, 0, 0], [0, 0, -1], [0, -1, 0]], dtype=np.float64)
+    pts[4, 0] = 2.0 ** -k
+    return pts
+
+
+def test_exact_capacity_predicate(cuda):
+    # 250 binades in one in_sphere call need more than the exact stage's 16
+    # limbs: a status, not a sign.  At 200 binades the sign is the reference's.
+    idx = np.array([[0, 1, 2, 3, 4]], np.int32)
+    ok = _wide_octahedron(200)
+    assert (d3.in_sphere(ok, idx) == oracle.ref_predicate("in_sphere", ok, idx)).all()
+    with pytest.raises(d3.Del3dError) as e:
+        d3.in_sphere(_wide_octahedron(250), idx)
+    assert e.value.status == d3.ERR_EXACT_CAPACITY
+    assert (d3.in_sphere(ok, idx) == oracle.ref_predicate("in_sphere", ok, idx)).all()
+
+
+def test_exact_capacity_build(cuda):
+    _expect(d3.ERR_EXACT_CAPACITY, _wide_octahedron(250))
+    _still_correct()
+    ok = _wide_octahedron(200)
+    d = d3.Delaunay()
+    d.build(ok)
+    assert np.array_equal(d.finite_cells(), oracle.canonical_cells(oracle.ref_build(ok)["cells"]))

@@ -111,3 +111,17 @@ def test_build_degenerate_no_cells():
         o = oracle.orc_build(pts)
         assert o["cells"].shape[0] == 0
     assert oracle.orc_build(np.tile([1.0, 2.0, 3.0], (20, 1)))["n_vertices"] == 1
+
+
+def test_oracle_workload_generators_match_the_library():
+    """The reference arm of bench.py draws its inputs from the oracle's copy of
+    the point generators (so it never loads libdel3d_b200.so); they must be the
+    product library's, bit for bit."""
+    import del3d_b200 as d3
+
+    ours = d3.mixed_workload(24, 32, 4096, seed=7, first_seed=300)
+    orc = oracle.mixed_workload(24, 32, 4096, seed=7, first_seed=300)
+    assert len(ours) == len(orc)
+    for a, b in zip(ours, orc):
+        assert a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    assert np.array_equal(d3.gen_uniform(1000, 6).view(np.uint64), oracle.gen_uniform(1000, 6).view(np.uint64))

@@ -101,3 +101,37 @@ def test_empty_and_invalid(cuda):
     assert d3.orient3d(pts, np.zeros((0, 4), np.int32)).shape == (0,)
     with pytest.raises(d3.Del3dError):
         d3.orient3d(pts, np.array([[0, 1, 2, 7]], np.int32))   # index out of range
+
+
+def test_lattice_sphere_groups_2m20(cuda):
+    """The predicate microbenchmark's degenerate groups: 5 points on a common
+    integer-lattice sphere of squared radius 1105^2 about a grid-aligned centre,
+    scaled by 2^-20 (exactly cospherical: the in_sphere tie-break decides), and
+    4 points on a common lattice plane (orient3d exactly zero), every rotation
+    of the point order."""
+    from bench import lattice_sphere_vectors
+
+    rng = np.random.default_rng(21)
+    vecs = lattice_sphere_vectors(1105 * 1105)
+    assert len(vecs) > 100 and (np.sum(vecs.astype(np.int64) ** 2, axis=1) == 1105 * 1105).all()
+    g5 = 400
+    centre = rng.integers(-(1 << 19), 1 << 19, (g5, 1, 3))
+    pick = np.stack([rng.choice(len(vecs), 5, replace=False) for _ in range(g5)])
+    sphere = ((centre + vecs[pick]).reshape(-1, 3) * 2.0 ** -20)
+    g4 = 400
+    a, b = rng.integers(-2, 3, (g4, 1)), rng.integers(-2, 3, (g4, 1))
+    k = rng.integers(-(1 << 17), 1 << 17, (g4, 1))
+    i, j = rng.integers(-(1 << 17), 1 << 17, (g4, 4)), rng.integers(-(1 << 17), 1 << 17, (g4, 4))
+    plane = np.stack([i, j, k - a * i - b * j], axis=2).reshape(-1, 3) * 2.0 ** -20
+    pts = np.concatenate([sphere, plane])
+    s_idx = np.concatenate([(np.arange(g5)[:, None] * 5 + (np.arange(5)[None, :] + r) % 5)
+                            for r in range(5)]).astype(np.int32)
+    o_idx = np.concatenate([(5 * g5 + np.arange(g4)[:, None] * 4 + (np.arange(4)[None, :] + r) % 4)
+                            for r in range(4)]).astype(np.int32)
+    got = d3.in_sphere(pts, s_idx)
+    assert (got != 0).all()
+    assert (got == oracle.ref_predicate("in_sphere", pts, s_idx)).all()
+    assert (got == oracle.exact_predicate("in_sphere", pts, s_idx)).all()
+    assert (d3.in_sphere_unperturbed(pts, s_idx) == 0).all()
+    o = d3.orient3d(pts, o_idx)
+    assert (o == 0).all() and (o == oracle.ref_predicate("orient3d", pts, o_idx)).all()

@@ -87,3 +87,33 @@ def test_noalloc_rejects_too_many_queries(cuda):
                                            d3.IN_SPHERE, out.data_ptr(), None, None)
     assert st == 1   # D3G_ERR_INVALID_ARGUMENT, before any device work
     assert b"D3G_NOALLOC_MAX_QUERIES" in lib.d3g_last_error()
+
+
+def test_noalloc_at_the_limit_matches_counts(cuda):
+    """Exactly D3G_NOALLOC_MAX_QUERIES in_sphere queries on points of one
+    integer-lattice sphere (squared radius 1105^2, scaled by 2^-20): every query
+    is exactly cospherical, so every one goes through the exact-stage queue in
+    the fixed array, filling it to its last element.  Signs and the exact-stage
+    count equal the allocating entry point's."""
+    import torch
+
+    from bench import lattice_sphere_vectors
+
+    lib = _lib()
+    rng = np.random.default_rng(9)
+    pts_h = lattice_sphere_vectors(1105 * 1105).astype(np.float64) * 2.0 ** -20
+    idx_h = rng.integers(0, len(pts_h), (MAX_QUERIES, 5)).astype(np.int32)
+    pts = torch.from_numpy(pts_h).to(cuda)
+    idx = torch.from_numpy(idx_h).to(cuda)
+    res = {}
+    for name in ("d3g_predicates_noalloc_device", "d3g_predicates_device"):
+        st = (ctypes.c_int64 * 2)()
+        out = torch.zeros(MAX_QUERIES, dtype=torch.int8, device=cuda)
+        rc = getattr(lib, name)(pts.data_ptr(), pts.shape[0], idx.data_ptr(), MAX_QUERIES, d3.IN_SPHERE,
+                                out.data_ptr(), None, ctypes.cast(st, ctypes.c_void_p))
+        assert rc == 0, lib.d3g_last_error().decode()
+        res[name] = (out.cpu().numpy(), st[0], st[1])
+    got, want = res["d3g_predicates_noalloc_device"], res["d3g_predicates_device"]
+    assert got[1] == want[1] == MAX_QUERIES
+    assert got[2] == want[2] == MAX_QUERIES, (got[2], want[2])
+    assert np.array_equal(got[0], want[0])
