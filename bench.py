@@ -58,7 +58,6 @@ import argparse
 import ctypes
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -366,19 +365,16 @@ def run_reference(args):
 # ---- ours ----------------------------------------------------------------------------
 
 
-def traffic_per_unit(kernel):
-    """DRAM bytes per unit of work of `kernel` from the committed ncu summary (a line
-    `` `<kernel>` dram bytes per <unit>: <number> ``), as (bytes, unit), or (None, None)."""
-    path = os.path.join(ROOT, "profiles", "traffic_per_attempt.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                m = re.search(rf"`{kernel}` dram bytes per ([a-z ]+): ([0-9.]+)", line)
-                if m:
-                    return float(m.group(2)), m.group(1)
-    except OSError:
-        pass
-    return None, None
+# Measured DRAM traffic of the insertion kernel per point it inserts, from the
+# one-kernel ncu capture summarised in profiles/k_insert_async_batched256_finest.md
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch / the points that
+# launch inserted; a 256-set case of this workload, whose traffic per inserted
+# point stays the same at full size: every insertion does the same work on a
+# table much larger than L2).
+INSERT_DRAM_BYTES_PER_POINT = 16463.0
+# Algorithmic bytes of the build per point: the coordinates read (24 B) plus the
+# finite tets written (6.75 per point x 16 B).
+BUILD_BYTES_PER_POINT = 24.0 + 6.75 * 16.0
 
 
 def plain_leg(torch, d3, x, offs, stream, out, sets_idx):
@@ -647,18 +643,21 @@ def run_ours(args):
         share = min(1.0, stats.get("async_inserted", 0) / inserted)
         if dom == "k_insert_async":
             Ca, Fa = C * share, F * share
-            bytes_kernel = 20 * (Ca + Fa) + 16 * Ca + 36 * Fa
+            model_bytes = 20 * (Ca + Fa) + 16 * Ca + 36 * Fa
             launches = max(1, stats.get("launches_async", 1))
+            units = stats.get("async_inserted", 0)
         else:
             Cr, Fr = C * (1 - share), F * (1 - share)
-            bytes_kernel = {"k_cavity": 24 * (Cr + Fr) + 16 * Cr, "k_check": 8 * (Cr + Fr) + 16 * Fr,
-                            "k_restar": 32 * Cr + 32 * Fr + 40 * Fr}[dom]
+            model_bytes = {"k_cavity": 24 * (Cr + Fr) + 16 * Cr, "k_check": 8 * (Cr + Fr) + 16 * Fr,
+                           "k_restar": 32 * Cr + 32 * Fr + 40 * Fr}[dom]
             launches = max(1, stats.get("launches_cavity", 1))
-        achieved = (bytes_kernel / launches) / (kern[dom] / launches / 1000.0) / 1e9 if kern[dom] else 0.0
-        per_unit, unit = traffic_per_unit(dom)
-        units = {"inserted point": stats.get("async_inserted", 0),
-                 "attempt": stats.get("attempts", 0) * (1 - share)}.get(unit, 0)
-        traffic = per_unit * units / launches if per_unit else None
+            units = inserted - stats.get("async_inserted", 0)
+        sec_per_launch = kern[dom] / launches / 1000.0 if kern[dom] else 0.0
+        # The survey's algorithmic bytes: 132 B per point the kernel inserts.
+        alg_bytes = BUILD_BYTES_PER_POINT * units / launches
+        achieved = alg_bytes / sec_per_launch / 1e9 if sec_per_launch else 0.0
+        model_achieved = (model_bytes / launches) / sec_per_launch / 1e9 if sec_per_launch else 0.0
+        traffic = INSERT_DRAM_BYTES_PER_POINT * units / launches if dom == "k_insert_async" else None
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
@@ -679,8 +678,17 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                          "traffic": traffic,
-                         "bytes_per_launch": bytes_kernel / launches,
-                         "ms_per_launch": kern[dom] / launches},
+                         "bytes_per_launch": alg_bytes, "points_per_launch": units / launches,
+                         "ms_per_launch": kern[dom] / launches,
+                         "bytes_definition": f"{BUILD_BYTES_PER_POINT:.0f} B per inserted point (24 B of "
+                                             "coordinates in, 6.75 finite tets x 16 B out)",
+                         "traffic_definition": f"{INSERT_DRAM_BYTES_PER_POINT:.0f} DRAM bytes per inserted "
+                                               "point measured by ncu x the points per launch",
+                         "builder_model": {"achieved": model_achieved, "frac": model_achieved / hbm,
+                                           "bytes_per_launch": model_bytes / launches,
+                                           "definition": "20 B per region and ring tet read (vertices "
+                                                         "+ lock), 16 B per region tet's neighbours, "
+                                                         "36 B per new tet written"}},
             "gpu_launches": (launches_per_step * args.steps) if launches_per_step else None,
             "clocks": clk,
             "build_stats": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in stats.items()},
@@ -697,6 +705,22 @@ def run_ours(args):
             line["cpu_baseline"] = cpu_baseline_leg(sets)
             line["parity"] = parity_leg(sets, par_cells)
     if rank == 0:
+        # The figures of the headline metric, last in the line.
+        srv = (line.get("serving") or {}).get("sweep") or []
+        p1e7 = line.get("plain_1e7") or {}
+        line["headline"] = {
+            "batched_points_per_s": value,
+            "e2e_points_per_s": e2e_value,
+            "plain_points_per_s": plain["points_per_s"] if plain else None,
+            "batched_over_plain": plain["batched_over_plain"] if plain else None,
+            "e2e_over_plain": (e2e_value / plain["points_per_s"]) if plain and e2e_value else None,
+            "plain_set_ms_p50": plain["latency_ms_p50"] if plain else None,
+            "plain_set_ms_p99": plain["latency_ms_p99"] if plain else None,
+            "serving_ms_p50_by_rate": {str(r["rate_req_per_s"]): r["latency_ms_p50"] for r in srv},
+            "serving_ms_p99_by_rate": {str(r["rate_req_per_s"]): r["latency_ms_p99"] for r in srv},
+            "plain_1e7_over_reference_1thread": p1e7.get("gpu_over_reference"),
+            "parity_equal": (line.get("parity") or {}).get("equal"),
+        }
         print(json.dumps(line))
     if dist:
         dist.barrier()

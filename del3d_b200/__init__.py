@@ -83,7 +83,9 @@ class BuildStats(ctypes.Structure):
                 ("ms_cavity", ctypes.c_double), ("ms_check", ctypes.c_double),
                 ("ms_restar", ctypes.c_double), ("launches_cavity", _I64),
                 ("walk_steps", _I64), ("bfs_steps", _I64), ("ms_async", ctypes.c_double),
-                ("launches_async", _I64), ("async_inserted", _I64)]
+                ("launches_async", _I64), ("async_inserted", _I64), ("conflict_tests", _I64),
+                ("uncertain_tests", _I64), ("tie_breaks", _I64), ("max_region_tets", _I64),
+                ("deferred_points", _I64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -102,7 +104,7 @@ class _Options(ctypes.Structure):
     _fields_ = [("want_all_cells", _I32), ("want_incident", _I32), ("chunk", _I32),
                 ("max_rounds", _I32), ("timing", _I32), ("alpha_small", _I32), ("split", _I32),
                 ("lanes", _I32), ("schedule", _I32), ("tet_capacity", _I32), ("walk_limit", _I32),
-                ("cavity_capacity", _I32)]
+                ("cavity_capacity", _I32), ("validate", _I32)]
 
 
 class _BatchResult(ctypes.Structure):
@@ -497,13 +499,14 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: Optional[int] = N
                  stats: Optional[dict] = None, alpha_small: Optional[int] = None, split: Optional[int] = None,
                  lanes: Optional[int] = None, schedule: Optional[int] = None, max_rounds: Optional[int] = None,
                  tet_capacity: Optional[int] = None, walk_limit: Optional[int] = None,
-                 cavity_capacity: Optional[int] = None):
+                 cavity_capacity: Optional[int] = None, validate: Optional[bool] = None):
     """Builds from a device-resident torch tensor (n, 3) float64 on `stream`
     (a raw cudaStream_t handle; 0 = default) and returns the canonical finite
     cells as a device int32 tensor view (n_cells, 4) and the vertex count.
     `out` may supply the (cap, 4) int32 output buffer.  Synchronises `stream`.
     max_rounds / tet_capacity / walk_limit / cavity_capacity lower the build's
-    limits (d3g_options), which makes their failure statuses reachable."""
+    limits (d3g_options), which makes their failure statuses reachable;
+    `validate` checks the device tet table's invariants after every level."""
     import torch
 
     lib = library()
@@ -517,7 +520,7 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: Optional[int] = N
     lib.d3g_options_default(ctypes.byref(opts))
     _apply(opts, chunk=chunk, timing=int(timing), alpha_small=alpha_small, split=split, lanes=lanes,
            schedule=schedule, max_rounds=max_rounds, tet_capacity=tet_capacity, walk_limit=walk_limit,
-           cavity_capacity=cavity_capacity)
+           cavity_capacity=cavity_capacity, validate=None if validate is None else int(validate))
     st = BuildStats()
     _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), out.shape[0],
                                 ctypes.byref(nc), ctypes.byref(nv), _P(stream), ctypes.byref(st)),
@@ -562,11 +565,12 @@ def build_batch(sets, chunk: int = 0, stats: Optional[dict] = None):
 def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk: Optional[int] = None,
                        stats: Optional[dict] = None, alpha_small: Optional[int] = None,
                        split: Optional[int] = None, lanes: Optional[int] = None,
-                       schedule: Optional[int] = None):
+                       schedule: Optional[int] = None, validate: Optional[bool] = None):
     """Device-resident form of build_batch: `points_dev` (n, 3) float64 CUDA
     tensor holding the sets back to back, `set_offsets` (n_sets + 1) host
     int64.  Returns the device cells tensor (all sets), the cell offsets per
-    set and the vertex counts per set.  Synchronises `stream`."""
+    set and the vertex counts per set.  Synchronises `stream`.  `validate`:
+    check the device tet table's invariants after every level (debug)."""
     import torch
 
     lib = library()
@@ -579,7 +583,8 @@ def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk
     nv = np.zeros(nsets, dtype=np.int64)
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
-    _apply(opts, chunk=chunk, alpha_small=alpha_small, split=split, lanes=lanes, schedule=schedule)
+    _apply(opts, chunk=chunk, alpha_small=alpha_small, split=split, lanes=lanes, schedule=schedule,
+           validate=None if validate is None else int(validate))
     st = BuildStats()
     _check(lib.d3g_build_batch_device(x.data_ptr(), _ptr(offs), nsets, ctypes.byref(opts), out.data_ptr(),
                                       out.shape[0], _ptr(co), _ptr(nv), _P(stream), ctypes.byref(st)),
@@ -916,8 +921,9 @@ def load_point_sets(paths, threads: int = 0):
 def validate_cells(all_cells, n_points: int = 0) -> None:
     """Checks all_cells() (infinite vertex -1) as the reference's Tds::validate()
     checks its cell table: distinct vertices in range, every facet shared by two
-    consistently oriented cells, Euler characteristic 0.  Raises Del3dError with
-    the first violation.  Host only."""
+    consistently oriented cells, Euler characteristic 0 - necessary conditions,
+    with no coordinates read (a complex flipped throughout, or not Delaunay,
+    passes).  Raises Del3dError with the first violation.  Host only."""
     t = np.ascontiguousarray(all_cells, dtype=np.int32).reshape(-1, 4)
     _check(library().d3g_validate_cells(_ptr(t) if t.shape[0] else None, t.shape[0], int(n_points)),
            "validate_cells")

@@ -132,7 +132,57 @@ struct Round {
     unsigned long long* steps;  // timing runs only (else null): [0] walk steps,
                                 // [1] breadth-first steps, over all attempts
     uint32_t* status;
+    unsigned long long* pstats; // [0] conflict tests, [1] of which the filter left uncertain,
+                                // [2] of which exactly degenerate (tie-break), [3] largest
+                                // conflict region inserted (tets)
 };
+
+/// A thread's conflict-test counters, added to Round::pstats once at the end
+/// of a launch (flush_counters).  `flags` holds the uncertain count in its low
+/// 20 bits and the tie count above: a thread makes far fewer than 2^20 tests in
+/// one launch (a warp inserts a few hundred points per launch, a few tests per
+/// lane each).  The insertion kernels keep them in shared memory, one slot per
+/// thread, so that they take no registers from the loops they count in.
+constexpr int kCounterThreads = 128;   // the insertion kernels' block size
+
+struct SharedCounters {
+    unsigned* tests;
+    unsigned* flags;
+    int* max_region;
+    __device__ void count(int r) const {
+        tests[threadIdx.x] += 1;
+        flags[threadIdx.x] += ((r >> 1) & 1) + (((r >> 2) & 1) << 20);
+    }
+    __device__ void region(int c) const { max_region[threadIdx.x] = max(max_region[threadIdx.x], c); }
+};
+
+#define D3G_SHARED_COUNTERS(name)                                                   \
+    __shared__ unsigned name##_t[kCounterThreads], name##_f[kCounterThreads];     \
+    __shared__ int name##_m[kCounterThreads];                                       \
+    name##_t[threadIdx.x] = 0;                                                      \
+    name##_f[threadIdx.x] = 0;                                                      \
+    name##_m[threadIdx.x] = 0;                                                      \
+    const SharedCounters name{name##_t, name##_f, name##_m}
+
+/// Sums the warp's counters into R.pstats (one atomic per counter per warp).
+__device__ void flush_counters(const SharedCounters& c, const Round& R) {
+    unsigned long long t = c.tests[threadIdx.x], u = c.flags[threadIdx.x] & 0xFFFFFu,
+                       z = c.flags[threadIdx.x] >> 20;
+    int m = c.max_region[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_xor_sync(0xffffffffu, t, o);
+        u += __shfl_xor_sync(0xffffffffu, u, o);
+        z += __shfl_xor_sync(0xffffffffu, z, o);
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (t) atomicAdd(R.pstats, t);
+        if (u) atomicAdd(R.pstats + 1, u);
+        if (z) atomicAdd(R.pstats + 2, z);
+        if (m) atomicMax(R.pstats + 3, (unsigned long long)m);
+    }
+}
 
 /// Claim key of point v this round: (~round) << 32 makes every newer round win
 /// against stale claims; the point rank breaks ties (earliest wins).
@@ -180,11 +230,32 @@ __device__ __noinline__ int hull_in_circle(double ax, double ay, double az, doub
     return coplanar_in_circle(Pt{ax, ay, az}, Pt{bx, by, bz}, Pt{dx, dy, dz}, Pt{px, py, pz}, id, st);
 }
 
-/// The reference's conflict test, src/triangulation.cpp:588-602.  `ex`: the
-/// point set's coordinates span few enough bits that the orient3d and in_sphere
-/// filters compute their determinants exactly.
-__device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __restrict__ vx, bool ex,
-                            uint32_t* st) {
+/// Outcome bits of a conflict test: in conflict; the floating-point filter
+/// could not certify the sign (the set's exact filter value, the exact stage or
+/// a tie-break decided it); the exact value was zero (decided by the symbolic
+/// perturbation, or the hull in-circle test); and, for the fast variant only,
+/// undecided (left to the full variant).
+enum : int { CT_IN = 1, CT_UNCERTAIN = 2, CT_TIE = 4, CT_UNDECIDED = 8 };
+
+/// in_sphere's exact sign for a set whose filter is not exact and, when it is
+/// zero, the reference's tie-break (src/predicates.cpp:206-232): the sign, plus
+/// 4 if the tie-break gave it.  Out of line.
+__device__ __noinline__ int in_sphere_exact_tie(double ax, double ay, double az, double bx, double by, double bz,
+                                                double cx, double cy, double cz, double dx, double dy, double dz,
+                                                double ex, double ey, double ez, int id0, int id1, int id2, int id3,
+                                                int id4, double fdet, uint32_t* st) {
+    const int s = in_sphere_degenerate(ax, ay, az, bx, by, bz, cx, cy, cz, dx, dy, dz, ex, ey, ez, id0, id1, id2, id3,
+                                       id4, fdet, 0, st);
+    if (s != 0) return s;
+    return 4 + in_sphere_perturb(Pt{ax, ay, az}, Pt{bx, by, bz}, Pt{cx, cy, cz}, Pt{dx, dy, dz}, Pt{ex, ey, ez},
+                                 id0, id1, id2, id3, id4, st);
+}
+
+/// The reference's conflict test, src/triangulation.cpp:588-602, with its
+/// outcome bits (CT_*).  `ex`: the point set's coordinates span few enough bits
+/// that the orient3d and in_sphere filters compute their determinants exactly.
+__device__ int conflict_test(const int4 t, const Pt& p, int pid, const double* __restrict__ vx, bool ex,
+                             uint32_t* st) {
     const int ip = inf_pos(t);
     if (ip >= 0) {
         // For each slot of the infinite vertex, the three finite vertices in
@@ -194,25 +265,31 @@ __device__ bool in_conflict(const int4 t, const Pt& p, int pid, const double* __
         const int o2 = ip == 0 ? 3 : (ip == 1 ? 0 : (ip == 2 ? 3 : 2));
         const int va = at(t, o0), vb = at(t, o1), vd = at(t, o2);
         const Pt a = vpt(vx, va), b = vpt(vx, vb), d = vpt(vx, vd);
-        const int s = orient3d_x(a, b, d, p, ex, st);
-        if (s != 0) return s > 0;
-        return hull_in_circle(a.x, a.y, a.z, b.x, b.y, b.z, d.x, d.y, d.z, p.x, p.y, p.z, va, vb, vd, pid, st) > 0;
+        const Orient3dFilter f = orient3d_filter(a, b, d, p);
+        const int unc = f.certain ? 0 : CT_UNCERTAIN;
+        const int s = (f.certain || ex) ? -sign_of(f.det) : orient3d_exact(a, b, d, p, f.det, st);
+        if (s != 0) return (s > 0 ? CT_IN : 0) | unc;
+        return (hull_in_circle(a.x, a.y, a.z, b.x, b.y, b.z, d.x, d.y, d.z, p.x, p.y, p.z, va, vb, vd, pid, st) > 0
+                    ? CT_IN : 0) | unc | CT_TIE;
     }
     const Pt a = vpt(vx, t.x), b = vpt(vx, t.y), c = vpt(vx, t.z), d = vpt(vx, t.w);
     const InSphereFilter f = in_sphere_filter(a, b, c, d, p);
-    if (f.certain || (ex && f.det != 0.0)) return f.det < 0.0;   // in_sphere = -sign(det)
+    if (f.certain) return f.det < 0.0 ? CT_IN : 0;   // in_sphere = -sign(det)
+    if (ex && f.det != 0.0) return (f.det < 0.0 ? CT_IN : 0) | CT_UNCERTAIN;
     if (ex)
-        return in_sphere_tiebreak_exact(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, p.x, p.y, p.z,
-                                        t.x, t.y, t.z, t.w, pid, st) > 0;
-    return in_sphere_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, p.x, p.y, p.z, t.x,
-                                t.y, t.z, t.w, pid, f.det, 1, st) > 0;
+        return (in_sphere_tiebreak_exact(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, p.x, p.y, p.z,
+                                         t.x, t.y, t.z, t.w, pid, st) > 0 ? CT_IN : 0) | CT_UNCERTAIN | CT_TIE;
+    const int r = in_sphere_exact_tie(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, p.x, p.y, p.z, t.x,
+                                      t.y, t.z, t.w, pid, f.det, st);
+    const bool tie = r > 1;
+    return ((tie ? r - 4 : r) > 0 ? CT_IN : 0) | CT_UNCERTAIN | (tie ? CT_TIE : 0);
 }
 
-/// in_conflict out of line, for the once-per-insertion seed check (one inline
-/// copy, in the breadth-first growth, is enough for the hot path).
-__device__ __noinline__ bool in_conflict_seed(int4 t, double px, double py, double pz, int pid,
-                                              const double* __restrict__ vx, bool ex, uint32_t* st) {
-    return in_conflict(t, Pt{px, py, pz}, pid, vx, ex, st);
+/// conflict_test out of line, for the once-per-insertion seed check (one inline
+/// copy, in the breadth-first growth, is enough).
+__device__ __noinline__ int conflict_test_seed(int4 t, double px, double py, double pz, int pid,
+                                               const double* __restrict__ vx, bool ex, uint32_t* st) {
+    return conflict_test(t, Pt{px, py, pz}, pid, vx, ex, st);
 }
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -334,6 +411,7 @@ template <int G>
 __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R, const double* __restrict__ vx,
                                                 int first) {
     const Lanes<G> L;
+    D3G_SHARED_COUNTERS(ctr);
     const int slot = first + int((blockIdx.x * blockDim.x + threadIdx.x) / G);
     bool live = slot < W.n;
     int w = 0, v = -1;
@@ -395,12 +473,16 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
                 kind = 3;                               // seen by us: decided below
             } else if ((old >> 1) < mine) {
                 abort = true;                           // an earlier point holds it
-            } else if (in_conflict(T.tv[nb], p, v, vx, ex, R.status)) {
-                const unsigned long long o2 = atomicMin(T.claim + nb, key);
-                if ((o2 >> 1) < mine) abort = true;
-                else kind = 2;
             } else {
-                kind = 1;
+                const int r = conflict_test(T.tv[nb], p, v, vx, ex, R.status);
+                ctr.count(r);
+                if (r & CT_IN) {
+                    const unsigned long long o2 = atomicMin(T.claim + nb, key);
+                    if ((o2 >> 1) < mine) abort = true;
+                    else kind = 2;
+                } else {
+                    kind = 1;
+                }
             }
         }
         const unsigned ab0 = L.own(__ballot_sync(kFull, abort));
@@ -451,6 +533,7 @@ __global__ void __launch_bounds__(128, 8) k_cavity(Tables T, Workers W, Round R,
         }
         __syncwarp();
     }
+    flush_counters(ctr, R);
 }
 
 /// One group per candidate: it wins if it still holds every claim it made.
@@ -479,7 +562,10 @@ __global__ void __launch_bounds__(128, 8) k_check(Tables T, Workers W, Round R, 
         }
     }
     const bool win = L.own(__ballot_sync(kFull, !ok)) == 0;
-    if (live && L.sub == 0) W.state[w] = win ? WS_WIN : WS_LOST;
+    if (live && L.sub == 0) {
+        W.state[w] = win ? WS_WIN : WS_LOST;
+        if (win) atomicMax(R.pstats + 3, (unsigned long long)W.ncav[w]);
+    }
 }
 
 /// Neighbour of new tet facet j (the new tet replaces facet i of region tet c):
@@ -652,7 +738,8 @@ struct AsyncCtx {
     int64_t stride;                 // chunk q of the queue is chunk (q * stride) % W.n
     unsigned long long* ekey;       // per warp slot: 3 edge keys per boundary facet (re-star)
     unsigned long long* stats;      // [0] lock conflicts, [1] walk restarts, [2] invalid seeds,
-                                    // [3] regions too big, [4] points left, [5] first points left
+                                    // [3] regions too big, [4] points left, [5] first points left,
+                                    // [6] points deferred by the fast variant
 };
 
 using LockRef = cuda::atomic_ref<int, cuda::thread_scope_device>;
@@ -673,9 +760,25 @@ __device__ __forceinline__ void unlock_if(int* lock, int t, int value) {
 
 __device__ __forceinline__ int4 ld4(const int4* p) { return __ldcg(p); }
 
+/// orient3d of tet (a, b, c, d) with vertex `i` replaced by p, from the filter
+/// alone: the sign when the filter decides it (or `ex`: the set's coordinates
+/// make the filter's value exact), else 2.  Selects, no calls and no local
+/// arrays, so that it adds nothing to the caller's live state.
+__device__ __forceinline__ int orient_replaced_filter(const Pt& a, const Pt& b, const Pt& c, const Pt& d, int i,
+                                                      const Pt& p, bool ex) {
+    const Pt A = i == 0 ? p : a, B = i == 1 ? p : b, C = i == 2 ? p : c, D = i == 3 ? p : d;
+    const Orient3dFilter f = orient3d_filter(A, B, C, D);
+    if (f.certain || ex) return -sign_of(f.det);
+    return 2;
+}
+
 /// Visibility walk on a mesh other warps are changing: reads go to L2 and may
 /// be stale, so the tet it returns is only a candidate, checked under its lock.
 /// Returns -1 after kAsyncWalkLimit steps (or the build's walk limit, if lower).
+/// kFast: orientations come from the filter alone, and a step the filter cannot
+/// decide ends the walk with -2 (the point is left to the other variant, which
+/// runs the exact stage).
+template <bool kFast>
 __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const double* __restrict__ vx,
                           bool ex, uint32_t* st, int lane) {
     int4 tv = ld4(T.tv + t);
@@ -693,12 +796,24 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
         const int4 tn = ld4(T.tn + t);
         h = h * 1664525u + 1013904223u;
         const int s0 = int(h >> 30);
-        bool neg = false;
+        bool neg = false, undecided = false;
         if (lane < 4 && (at(tn, lane) >> 2) != prev && tv.x != kInf && tv.y != kInf && tv.z != kInf &&
             tv.w != kInf) {
-            const Pt q[4] = {vpt(vx, tv.x), vpt(vx, tv.y), vpt(vx, tv.z), vpt(vx, tv.w)};
-            neg = orient_replaced(q, lane, p, ex, st) < 0;
+            const Pt a = vpt(vx, tv.x), b = vpt(vx, tv.y), c = vpt(vx, tv.z), d = vpt(vx, tv.w);
+            int o = orient_replaced_filter(a, b, c, d, lane, p, ex);
+            if (o == 2) {
+                if (kFast) {
+                    undecided = true;
+                    o = 0;
+                } else {
+                    const Pt A = lane == 0 ? p : a, B = lane == 1 ? p : b, C = lane == 2 ? p : c,
+                             D = lane == 3 ? p : d;
+                    o = orient3d(A, B, C, D, st);
+                }
+            }
+            neg = o < 0;
         }
+        if (kFast && __any_sync(kFull, undecided)) return -2;
         const unsigned m = __ballot_sync(kFull, neg) & 0xFu;
         if (m == 0) return t;
         const unsigned rot = ((m >> s0) | (m << (4 - s0))) & 0xFu;
@@ -713,7 +828,145 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
     return -1;
 }
 
-enum : int { AI_DONE = 0, AI_RETRY = 1, AI_LEAVE = 2 };
+/// A vertex coordinate read again from memory (the read-only path), as a
+/// volatile load so that the compiler does not keep an earlier read of it
+/// alive in registers across the code in between.
+__device__ __forceinline__ double ld_coord(const double* p) {
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ Pt ld_vertex(const double* __restrict__ vx, int v) {
+    const double* q = vx + 3 * int64_t(v);
+    return Pt{ld_coord(q), ld_coord(q + 1), ld_coord(q + 2)};
+}
+
+/// The symbolic perturbation of an exactly cospherical in_sphere(a, b, c, d, p)
+/// (reference src/predicates.cpp:206-232) for the conflict test of tet t and
+/// vertex pid, when the set's coordinates make the orient3d filter exact.  The
+/// five points are distinct vertices, so their lexicographic order is strict:
+/// walking down it from the largest, the largest is p -> NEGATIVE; else the
+/// orient3d with that point's slot replaced by p decides if it is not zero;
+/// else the next largest, once more; else NEGATIVE.  Points are read again
+/// from memory each time they are needed, so the tie-break adds no live state
+/// to the loop around it.
+__device__ __forceinline__ int in_sphere_tiebreak_ex(const int4 t, int pid, const double* __restrict__ vx) {
+    int skip = -1;
+#pragma unroll 1
+    for (int r = 0; r < 2; ++r) {
+        int best = -1;
+        Pt bp{0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int k = 0; k < 5; ++k) {
+            if (k == skip) continue;
+            const Pt q = ld_vertex(vx, k < 4 ? at(t, k) : pid);
+            if (best < 0 || lexico_less(bp, q)) {
+                best = k;
+                bp = q;
+            }
+        }
+        if (best == 4) return -1;
+        const Pt pp = ld_vertex(vx, pid);
+        const Pt A = best == 0 ? pp : ld_vertex(vx, t.x), B = best == 1 ? pp : ld_vertex(vx, t.y),
+                 C = best == 2 ? pp : ld_vertex(vx, t.z), D = best == 3 ? pp : ld_vertex(vx, t.w);
+        const int o = -sign_of(orient3d_filter(A, B, C, D).det);
+        if (o != 0) return o;
+        skip = best;
+    }
+    return -1;
+}
+
+/// in_sphere_filter's arithmetic, operation for operation (so its value and
+/// its decision are bit-identical), in an order that retires values early:
+/// lifts right after the differences, each product pair folded at once into
+/// its minor and its permanent pair sum (|x*y| = |x|*|y| exactly).
+__device__ __forceinline__ InSphereFilter in_sphere_filter_lean(const Pt& a, const Pt& b, const Pt& c, const Pt& d,
+                                                                const Pt& e) {
+    const double aex = fsub(a.x, e.x), aey = fsub(a.y, e.y), aez = fsub(a.z, e.z);
+    const double bex = fsub(b.x, e.x), bey = fsub(b.y, e.y), bez = fsub(b.z, e.z);
+    const double cex = fsub(c.x, e.x), cey = fsub(c.y, e.y), cez = fsub(c.z, e.z);
+    const double dex = fsub(d.x, e.x), dey = fsub(d.y, e.y), dez = fsub(d.z, e.z);
+    const double alift = fadd(fadd(fmul(aex, aex), fmul(aey, aey)), fmul(aez, aez));
+    const double blift = fadd(fadd(fmul(bex, bex), fmul(bey, bey)), fmul(bez, bez));
+    const double clift = fadd(fadd(fmul(cex, cex), fmul(cey, cey)), fmul(cez, cez));
+    const double dlift = fadd(fadd(fmul(dex, dex), fmul(dey, dey)), fmul(dez, dez));
+    double ab, bc, cd, da, ac, bd, sab, sbc, scd, sda, sac, sbd;
+    {
+        const double p = fmul(aex, bey), q = fmul(bex, aey);
+        ab = fsub(p, q);
+        sab = fadd(fabs_(p), fabs_(q));
+    }
+    {
+        const double p = fmul(bex, cey), q = fmul(cex, bey);
+        bc = fsub(p, q);
+        sbc = fadd(fabs_(p), fabs_(q));
+    }
+    {
+        const double p = fmul(cex, dey), q = fmul(dex, cey);
+        cd = fsub(p, q);
+        scd = fadd(fabs_(p), fabs_(q));
+    }
+    {
+        const double p = fmul(dex, aey), q = fmul(aex, dey);
+        da = fsub(p, q);
+        sda = fadd(fabs_(p), fabs_(q));
+    }
+    {
+        const double p = fmul(aex, cey), q = fmul(cex, aey);
+        ac = fsub(p, q);
+        sac = fadd(fabs_(p), fabs_(q));
+    }
+    {
+        const double p = fmul(bex, dey), q = fmul(dex, bey);
+        bd = fsub(p, q);
+        sbd = fadd(fabs_(p), fabs_(q));
+    }
+    const double abc = fadd(fsub(fmul(aez, bc), fmul(bez, ac)), fmul(cez, ab));
+    const double bcd = fadd(fsub(fmul(bez, cd), fmul(cez, bd)), fmul(dez, bc));
+    const double cda = fadd(fadd(fmul(cez, da), fmul(dez, ac)), fmul(aez, cd));
+    const double dab = fadd(fadd(fmul(dez, ab), fmul(aez, bd)), fmul(bez, da));
+    const double det = fadd(fsub(fmul(dlift, abc), fmul(clift, dab)), fsub(fmul(blift, cda), fmul(alift, bcd)));
+    const double aezp = fabs_(aez), bezp = fabs_(bez), cezp = fabs_(cez), dezp = fabs_(dez);
+    const double pa = fadd(fadd(fmul(scd, bezp), fmul(sbd, cezp)), fmul(sbc, dezp));
+    const double pb = fadd(fadd(fmul(sda, cezp), fmul(sac, dezp)), fmul(scd, aezp));
+    const double pc = fadd(fadd(fmul(sab, dezp), fmul(sbd, aezp)), fmul(sda, bezp));
+    const double pd = fadd(fadd(fmul(sbc, aezp), fmul(sac, bezp)), fmul(sab, cezp));
+    const double permanent = fadd(fadd(fadd(fmul(pa, alift), fmul(pb, blift)), fmul(pc, clift)), fmul(pd, dlift));
+    const double errbound = fmul(kInSphereBound, permanent);
+    InSphereFilter r;
+    r.det = det;
+    r.certain = (det > errbound) || (-det > errbound);
+    return r;
+}
+
+/// The conflict test of the fast variant (reference src/triangulation.cpp:588-602,
+/// as conflict_test), with its outcome bits; CT_UNDECIDED when the filter cannot
+/// decide and the exact stage is needed, or the point lies in the plane of a
+/// hull facet (the coplanar in-circle test).  Call-free: an exactly cospherical
+/// call on a set whose coordinates make the filter exact gets its tie-break
+/// inline.
+__device__ __forceinline__ int in_conflict_fast(const int4 t, const Pt& p, int pid, const double* __restrict__ vx,
+                                                bool ex) {
+    const int ip = inf_pos(t);
+    if (ip >= 0) {
+        const int o0 = ip == 0 ? 2 : (ip == 1 ? 2 : (ip == 2 ? 1 : 0));
+        const int o1 = ip == 0 ? 1 : (ip == 1 ? 3 : (ip == 2 ? 0 : 1));
+        const int o2 = ip == 0 ? 3 : (ip == 1 ? 0 : (ip == 2 ? 3 : 2));
+        const Pt a = vpt(vx, at(t, o0)), b = vpt(vx, at(t, o1)), d = vpt(vx, at(t, o2));
+        const Orient3dFilter f = orient3d_filter(a, b, d, p);
+        if (f.certain) return f.det < 0.0 ? CT_IN : 0;   // orient3d = -sign(det)
+        if (ex && f.det != 0.0) return (f.det < 0.0 ? CT_IN : 0) | CT_UNCERTAIN;
+        return CT_UNDECIDED;
+    }
+    const Pt a = vpt(vx, t.x), b = vpt(vx, t.y), c = vpt(vx, t.z), d = vpt(vx, t.w);
+    const InSphereFilter f = in_sphere_filter_lean(a, b, c, d, p);
+    if (f.certain) return f.det < 0.0 ? CT_IN : 0;   // in_sphere = -sign(det)
+    if (ex && f.det != 0.0) return (f.det < 0.0 ? CT_IN : 0) | CT_UNCERTAIN;
+    if (ex) return (in_sphere_tiebreak_ex(t, pid, vx) > 0 ? CT_IN : 0) | CT_UNCERTAIN | CT_TIE;
+    return CT_UNDECIDED;
+}
+
+enum : int { AI_DONE = 0, AI_RETRY = 1, AI_LEAVE = 2, AI_DEFER = 3 };
 
 /// Key of the edge (a, b), either order.
 __device__ __forceinline__ unsigned long long edge_key(int a, int b) {
@@ -734,14 +987,29 @@ __device__ __forceinline__ void facet_edge_keys(const int4 c, int i, unsigned lo
 
 /// One insertion of point v by the whole warp, starting the walk at tet t0.
 /// AI_DONE: inserted; AI_RETRY: a lock was taken by another warp (nothing
-/// changed, every lock given back); AI_LEAVE: leave it for the rounds.
+/// changed, every lock given back); AI_LEAVE: leave it for the rounds;
+/// AI_DEFER (kFast only): a test the filter could not decide, nothing changed,
+/// leave it for the other variant.
+///
+/// kFast = true is the variant for the bulk of the points: its walk and
+/// conflict tests use the filters alone and make no calls.  A call anywhere in
+/// the insertion loop - even one the uniform case never takes - makes the
+/// compiler keep the loop's state in local memory around it; without calls the
+/// state stays in registers.  kFast = false runs the exact stage, the hull
+/// in-circle test and the tie-breaks, out of line, for the points the fast
+/// variant deferred.
+template <bool kFast>
 __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, const AsyncCtx& A,
                             const double* __restrict__ vx, bool ex, uint32_t* st, int slot, int lane,
-                            unsigned long long* nC, unsigned long long* nF) {
+                            unsigned long long* nC, unsigned long long* nF, const SharedCounters& ctr) {
     const int owner = slot + 1;
     const int region = owner << 1, ring = region | 1;
     const Pt p = vpt(vx, v);
-    const int seed = walk_async(t0, p, v, T, vx, ex, st, lane);
+    const int seed = walk_async<kFast>(t0, p, v, T, vx, ex, st, lane);
+    if (kFast && seed == -2) {
+        if (lane == 0) atomicAdd(A.stats + 6, 1ull);
+        return AI_DEFER;
+    }
     if (seed < 0) {
         if (lane == 0) atomicAdd(A.stats + 1, 1ull);
         return AI_RETRY;
@@ -749,22 +1017,30 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
     int* cav = W.cav + int64_t(slot) * W.cav_cap;
     int* fac = W.fac + int64_t(slot) * W.fac_cap;
     // Seed: lock it, then check under the lock that it is alive and in conflict.
-    int res = 0;   // 0 ok, 1 lock held by another, 2 not a valid seed
+    int res = 0;   // 0 ok, 1 lock held by another, 2 not a valid seed, 3 undecided (kFast)
     if (lane == 0) {
         int seen = 0;
         if (!try_lock(A.lock, seed, region, &seen)) {
             res = 1;
-        } else if (!__ldcg(T.alive + seed) || !in_conflict_seed(ld4(T.tv + seed), p.x, p.y, p.z, v, vx, ex, st)) {
-            unlock_if(A.lock, seed, region);
-            res = 2;
         } else {
-            cav[0] = seed;
+            int r = 0;
+            if (__ldcg(T.alive + seed)) {
+                if (kFast) r = in_conflict_fast(ld4(T.tv + seed), p, v, vx, ex);
+                else r = conflict_test_seed(ld4(T.tv + seed), p.x, p.y, p.z, v, vx, ex, st);
+                ctr.count(r);
+            }
+            if (r & CT_IN) {
+                cav[0] = seed;
+            } else {
+                unlock_if(A.lock, seed, region);
+                res = (r & CT_UNDECIDED) ? 3 : 2;
+            }
         }
     }
     res = __shfl_sync(kFull, res, 0);
     if (res != 0) {
-        if (lane == 0) atomicAdd(A.stats + (res == 1 ? 0 : 2), 1ull);
-        return AI_RETRY;
+        if (lane == 0) atomicAdd(A.stats + (res == 1 ? 0 : (res == 2 ? 2 : 6)), 1ull);
+        return res == 3 ? AI_DEFER : AI_RETRY;
     }
     __syncwarp();
     const unsigned lt = (1u << lane) - 1u;
@@ -775,18 +1051,23 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         const bool valid = (lane >> 2) < nproc;
         const int i = lane & 3;
         int c = 0, nb = 0, kind = 0, got = -1;   // got: a tet this lane locked in this step
-        bool abort = false;
+        bool abort = false, undecided = false;
         if (valid) {
             c = cav[head + (lane >> 2)];
             nb = at(ld4(T.tn + c), i) >> 2;
             int seen = 0;
             if (try_lock(A.lock, nb, ring, &seen)) {
                 got = nb;
-                if (in_conflict(ld4(T.tv + nb), p, v, vx, ex, st)) {
+                int r;
+                if (kFast) r = in_conflict_fast(ld4(T.tv + nb), p, v, vx, ex);
+                else r = conflict_test(ld4(T.tv + nb), p, v, vx, ex, st);
+                ctr.count(r);
+                if (r & CT_IN) {
                     LockRef(A.lock[nb]).store(region, cuda::memory_order_relaxed);
                     kind = 2;
                 } else {
-                    kind = 1;
+                    kind = 1;                             // undecided: held as ring
+                    undecided = (r & CT_UNDECIDED) != 0;
                 }
             } else if (seen == region) {
                 kind = 0;                                 // already in the region
@@ -799,10 +1080,11 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         __syncwarp();
         if (kind == 3) kind = __ldcg(A.lock + nb) == region ? 0 : 1;
         const bool ab = __any_sync(kFull, abort);
+        const bool und = kFast && __any_sync(kFull, undecided);
         const unsigned mc = __ballot_sync(kFull, kind == 2);
         const unsigned mf = __ballot_sync(kFull, kind == 1);
         const bool full = ncav + __popc(mc) > W.cav_cap || nfac + __popc(mf) > W.fac_cap;
-        if (ab || full) {
+        if (ab || full || und) {
             // Give everything back: this step's new locks, the region, the ring.
             if (got >= 0) unlock_if(A.lock, got, kind == 2 ? region : ring);
             __syncwarp();
@@ -812,8 +1094,8 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             }
             __syncwarp();
             for (int k = lane; k < ncav; k += 32) unlock_if(A.lock, cav[k], region);
-            if (lane == 0) atomicAdd(A.stats + (ab ? 0 : 3), 1ull);
-            outcome = ab ? AI_RETRY : AI_LEAVE;
+            if (lane == 0) atomicAdd(A.stats + (ab ? 0 : (und ? 6 : 3)), 1ull);
+            outcome = ab ? AI_RETRY : (und ? AI_DEFER : AI_LEAVE);
             break;
         }
         if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
@@ -961,16 +1243,21 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         *nC += (unsigned long long)C;
         *nF += (unsigned long long)F;
     }
+    if (ok && lane == 0) ctr.region(C);
     return ok ? AI_DONE : AI_LEAVE;
 }
 
-/// Persistent warps over a level's chunks (set up by k_setup_level).
+/// Persistent warps over a level's chunks (set up by k_setup_level), or over
+/// the points a pass left, one worker each (k_setup_list).  kFast: the call-free
+/// variant; a point it cannot decide goes to A.leftover for the other variant.
+template <bool kFast>
 __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, AsyncCtx A, Round R,
                                                       const double* __restrict__ vx, int nslots) {
     const int lane = threadIdx.x & 31;
     const int slot = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (slot >= nslots) return;   // the grid is rounded up to whole blocks; scratch has nslots slots
     unsigned long long won = 0, tries = 0, nC = 0, nF = 0;
+    D3G_SHARED_COUNTERS(ctr);
     for (;;) {
         int q = 0;
         if (lane == 0) q = atomicAdd(A.next, 1);
@@ -989,7 +1276,7 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
             for (int attempt = 0; attempt < kAsyncRetries && outcome == AI_RETRY; ++attempt) {
                 if (attempt > 0) __nanosleep(200u << min(attempt, 6));
                 const int t0 = __ldcg(T.vert_tet + (last >= 0 ? last : guide));
-                outcome = insert_async(v, t0, T, W, A, vx, ex, R.status, slot, lane, &nC, &nF);
+                outcome = insert_async<kFast>(v, t0, T, W, A, vx, ex, R.status, slot, lane, &nC, &nF, ctr);
                 ++tries;
                 if (__ldcg(R.status) != 0) outcome = AI_LEAVE;
             }
@@ -1021,6 +1308,93 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
         atomicAdd(R.totals + 1, tries);
         atomicAdd(R.sums, nC);
         atomicAdd(R.sums + 1, nF);
+    }
+    flush_counters(ctr, R);
+}
+
+// ---- structural self-check (the reference's Tds::validate, src/tds.h:483-530) ----
+
+/// Codes of the first broken invariant k_validate finds.
+enum : int {
+    VF_VERTEX = 1,      // a vertex out of range, or repeated in a tet, or two infinite
+    VF_NEIGHBOUR = 2,   // a neighbour out of range or dead
+    VF_BACK = 3,        // a neighbour that does not point back through the same facet
+    VF_FACET = 4,       // two neighbours whose shared facets have different vertices
+    VF_LOCK = 5,        // a tet still locked after the asynchronous passes
+    VF_VERT_TET = 6,    // an inserted vertex whose tet is dead or does not contain it
+};
+
+/// One thread per tet slot, then one per vertex: checks what the reference's
+/// validate() checks - distinct vertices, live neighbours that point back, no
+/// mark left behind (here: no lock held), every vertex's cached tet alive and
+/// containing it - and, beyond it, that each pair of neighbours shares the
+/// same three vertices.  Every index is range-checked before it is followed.
+/// The first failure (lowest code, then lowest slot) is recorded in `fail` =
+/// code << 60 | tet or vertex << 30 | detail, and ST_INTERNAL is reported;
+/// nothing traps.
+__global__ void k_validate(Tables T, const int* __restrict__ lock, int ntet, int nv, uint32_t* status,
+                           unsigned long long* fail) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    int code = 0, where = 0, detail = 0;
+    if (i < ntet) {
+        const int c = int(i);
+        if (T.alive[c]) {
+            const int4 tv = T.tv[c], tn = T.tn[c];
+            int ninf = 0;
+            for (int k = 0; k < 4 && !code; ++k) {
+                const int v = at(tv, k);
+                if (v < -1 || v >= nv) code = VF_VERTEX;
+                ninf += v == kInf;
+                for (int m = k + 1; m < 4; ++m)
+                    if (v == at(tv, m)) code = VF_VERTEX;
+                detail = k;
+            }
+            if (!code && ninf > 1) code = VF_VERTEX;
+            for (int k = 0; k < 4 && !code; ++k) {
+                detail = k;
+                const int e = at(tn, k);
+                const int n = e >> 2, f = e & 3;
+                if (e < 0 || n >= ntet || !T.alive[n]) {
+                    code = VF_NEIGHBOUR;
+                    break;
+                }
+                if (at(T.tn[n], f) != c * 4 + k) {
+                    code = VF_BACK;
+                    break;
+                }
+                // The facet of c opposite k and the facet of n opposite f: the same
+                // three vertices (in any order).
+                const int4 nvx = T.tv[n];
+                for (int m = 0; m < 4 && !code; ++m) {
+                    if (m == k) continue;
+                    const int v = at(tv, m);
+                    bool found = false;
+                    for (int q = 0; q < 4; ++q) found = found || (q != f && at(nvx, q) == v);
+                    if (!found) code = VF_FACET;
+                }
+            }
+            if (!code && lock && lock[c] != 0) {
+                code = VF_LOCK;
+                detail = lock[c];
+            }
+        }
+        where = c;
+    } else if (i < int64_t(ntet) + nv) {
+        const int v = int(i - ntet);
+        const int c = T.vert_tet[v];
+        if (c >= 0) {   // -1: not inserted yet
+            if (c >= ntet || !T.alive[c]) code = VF_VERT_TET;
+            else if (pos_of(T.tv[c], v) == 3 && T.tv[c].w != v) code = VF_VERT_TET;
+            detail = c;
+        }
+        where = v;
+    }
+    if (code) {
+        report(status, ST_INTERNAL);
+        const unsigned long long rec = (unsigned long long)(uint32_t(code)) << 60 |
+                                       (unsigned long long)(uint32_t(where) & 0x3FFFFFFFu) << 30 |
+                                       (unsigned long long)(uint32_t(detail) & 0x3FFFFFFFu);
+        atomicMin(fail, rec);
     }
 }
 
@@ -1954,24 +2328,57 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     Rd.steps = opt.timing ? steps.p : nullptr;
     Rd.round = dround.p;
     Rd.status = status.p;
+    DevBuf<unsigned long long> pstats;
+    D3G_TRY(pstats.alloc(4, s));
+    D3G_CUDA(cudaMemsetAsync(pstats.p, 0, 4 * sizeof(unsigned long long), s));
+    Rd.pstats = pstats.p;
     const int max_rounds = opt.max_rounds > 0 ? opt.max_rounds : (1 << 20);
     int round = 0;
     // Asynchronous passes (see k_insert_async): a persistent grid of at most
-    // kAsyncWarps warps per level; the rounds finish what it leaves.
+    // kAsyncWarps warps per level, the fast variant over the level's chunks,
+    // the full variant over what that leaves; the rounds finish the rest.
     const bool use_async = opt.schedule != 1 && !grow;
     constexpr int kAsyncWarps = kNumSMs * 32;   // resident at 64 registers a thread
-    DevBuf<int> alock, anext, aleft, anleft;
+    DevBuf<int> alock, anext, aleft, aleft2, anleft;
     DevBuf<unsigned long long> astats, aekey;
     if (use_async) {
         D3G_TRY(aekey.alloc(size_t(std::min(maxw, kAsyncWarps)) * 3 * size_t(W.fac_cap), s));
         D3G_TRY(alock.alloc(size_t(T.cap), s));
         D3G_TRY(anext.alloc(1, s));
         D3G_TRY(aleft.alloc(size_t(nv), s));
-        D3G_TRY(anleft.alloc(1, s));
-        D3G_TRY(astats.alloc(6, s));
+        D3G_TRY(aleft2.alloc(size_t(nv), s));
+        D3G_TRY(anleft.alloc(2, s));
+        D3G_TRY(astats.alloc(7, s));
         D3G_CUDA(cudaMemsetAsync(alock.p, 0, sizeof(int) * size_t(T.cap), s));
-        D3G_CUDA(cudaMemsetAsync(astats.p, 0, 6 * sizeof(unsigned long long), s));
+        D3G_CUDA(cudaMemsetAsync(astats.p, 0, 7 * sizeof(unsigned long long), s));
     }
+    // Structural self-check after each level (opt.validate): k_validate over
+    // every tet slot and vertex; the first broken invariant ends the build.
+    DevBuf<unsigned long long> vfail;
+    auto validate_tables = [&](const char* when, int lev) -> int {
+        if (!vfail.p) D3G_TRY(vfail.alloc(1, s));
+        D3G_CUDA(cudaMemsetAsync(vfail.p, 0xFF, sizeof(unsigned long long), s));
+        int ntet_now = 0;
+        D3G_CUDA(cudaMemcpyAsync(&ntet_now, tet_count.p, sizeof ntet_now, cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));
+        const int64_t threads = int64_t(ntet_now) + nv;
+        k_validate<<<grid_for(threads, 256, 1 << 30), 256, 0, s>>>(T, use_async ? alock.p : nullptr, ntet_now, nv,
+                                                                   status.p, vfail.p);
+        D3G_CUDA(cudaGetLastError());
+        unsigned long long rec = ~0ull;
+        D3G_CUDA(cudaMemcpyAsync(&rec, vfail.p, sizeof rec, cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));
+        if (rec == ~0ull) return D3G_OK;
+        static const char* what[] = {"", "bad vertex", "bad neighbour", "neighbour does not point back",
+                                     "neighbours' shared facets differ", "lock held", "vertex's tet"};
+        const int code = int(rec >> 60);
+        char msg[200];
+        std::snprintf(msg, sizeof msg, "d3g_build: validate %s level %d: %s (%s %lld, %lld)", when, lev,
+                      what[code > 0 && code < 7 ? code : 0], code == VF_VERT_TET ? "vertex" : "tet",
+                      (long long)((rec >> 30) & 0x3FFFFFFFull), (long long)(rec & 0x3FFFFFFFull));
+        set_error(msg);
+        return D3G_ERR_INTERNAL;
+    };
     const bool trace = getenv("D3G_TRACE") != nullptr;
     cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};
     if (opt.timing)
@@ -2178,54 +2585,74 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         }
         return D3G_OK;
         };
-        long long async_left = -1;
+        long long async_left = -1, deferred = -1;
         if (use_async) {
-            // The chunks go out in a scattered order (stride coprime with the
-            // chunk count, near the golden ratio of it), so that chunks taken
-            // at the same time lie far apart along the curve.
-            int64_t stride = std::max<int64_t>(1, int64_t(double(W.n) * 0.6180339887));
-            while (std::gcd(stride, int64_t(W.n)) != 1) ++stride;
-            D3G_CUDA(cudaMemsetAsync(anext.p, 0, sizeof(int), s));
-            D3G_CUDA(cudaMemsetAsync(anleft.p, 0, sizeof(int), s));
-            AsyncCtx A{alock.p, anext.p, aleft.p, anleft.p, stride, aekey.p, astats.p};
-            const int warps = std::min(W.n, kAsyncWarps);
-            unsigned long long won0 = 0;
-            D3G_CUDA(cudaMemcpyAsync(&won0, totals.p, sizeof won0, cudaMemcpyDeviceToHost, s));
-            if (opt.timing) cudaEventRecord(kev[0], s);
-            k_insert_async<<<unsigned((int64_t(warps) * 32 + 127) / 128), 128, 0, s>>>(T, W, A, Rd, vx.p,
-                                                                                      warps);
-            D3G_CUDA(cudaGetLastError());
-            if (opt.timing) cudaEventRecord(kev[1], s);
-            int nleft = 0;
-            uint32_t hs = 0;
-            unsigned long long won1 = 0;
-            D3G_CUDA(cudaMemcpyAsync(&nleft, anleft.p, sizeof nleft, cudaMemcpyDeviceToHost, s));
-            D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
-            D3G_CUDA(cudaMemcpyAsync(&won1, totals.p, sizeof won1, cudaMemcpyDeviceToHost, s));
-            D3G_CUDA(cudaStreamSynchronize(s));
-            R.stats.launches_async += 1;
-            R.stats.async_inserted += int64_t(won1 - won0);
-            if (opt.timing) {
-                float am = 0.f;
-                cudaEventElapsedTime(&am, kev[0], kev[1]);
-                R.stats.ms_async += am;
-            }
-            if (hs != 0) {
-                const int st = status_from_bits(hs);
-                if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");
-                return st;
-            }
-            async_left = nleft;
-            // What the pass left goes through the rounds, maxw points at a time.
+            // One asynchronous pass: a persistent grid over the workers W
+            // (level chunks, or one leftover point each), writing the points it
+            // leaves to `left` / `nleft_d`; their count goes to *nleft_out.
+            auto async_pass = [&](bool fast, int* left, int* nleft_d, int* nleft_out) -> int {
+                // The chunks go out in a scattered order (stride coprime with the
+                // chunk count, near the golden ratio of it), so that chunks taken
+                // at the same time lie far apart along the curve.
+                int64_t stride = std::max<int64_t>(1, int64_t(double(W.n) * 0.6180339887));
+                while (std::gcd(stride, int64_t(W.n)) != 1) ++stride;
+                D3G_CUDA(cudaMemsetAsync(anext.p, 0, sizeof(int), s));
+                AsyncCtx A{alock.p, anext.p, left, nleft_d, stride, aekey.p, astats.p};
+                const int warps = std::min(W.n, kAsyncWarps);
+                const unsigned grid = unsigned((int64_t(warps) * 32 + 127) / 128);
+                unsigned long long won0 = 0;
+                D3G_CUDA(cudaMemcpyAsync(&won0, totals.p, sizeof won0, cudaMemcpyDeviceToHost, s));
+                if (opt.timing) cudaEventRecord(kev[0], s);
+                if (fast) k_insert_async<true><<<grid, 128, 0, s>>>(T, W, A, Rd, vx.p, warps);
+                else k_insert_async<false><<<grid, 128, 0, s>>>(T, W, A, Rd, vx.p, warps);
+                D3G_CUDA(cudaGetLastError());
+                if (opt.timing) cudaEventRecord(kev[1], s);
+                uint32_t hs = 0;
+                unsigned long long won1 = 0;
+                D3G_CUDA(cudaMemcpyAsync(nleft_out, nleft_d, sizeof(int), cudaMemcpyDeviceToHost, s));
+                D3G_CUDA(cudaMemcpyAsync(&hs, status.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+                D3G_CUDA(cudaMemcpyAsync(&won1, totals.p, sizeof won1, cudaMemcpyDeviceToHost, s));
+                D3G_CUDA(cudaStreamSynchronize(s));
+                R.stats.launches_async += 1;
+                R.stats.async_inserted += int64_t(won1 - won0);
+                if (opt.timing) {
+                    float am = 0.f;
+                    cudaEventElapsedTime(&am, kev[0], kev[1]);
+                    R.stats.ms_async += am;
+                }
+                if (hs != 0) {
+                    const int st = status_from_bits(hs);
+                    if (st == D3G_ERR_OOM) set_error("d3g_build: tet table full");
+                    return st;
+                }
+                return D3G_OK;
+            };
+            // The level's chunks through the fast variant; what it deferred or
+            // left (undecided tests, lock conflicts, regions too big) through
+            // the full variant, one worker per point, maxw points at a time;
+            // what that leaves through the rounds.
+            int nleft = 0, nleft2 = 0;
+            D3G_CUDA(cudaMemsetAsync(anleft.p, 0, 2 * sizeof(int), s));
+            D3G_TRY(async_pass(true, aleft.p, anleft.p, &nleft));
+            deferred = nleft;
             for (int off = 0; off < nleft; off += maxw) {
                 W.n = std::min(maxw, nleft - off);
                 k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, aleft.p + off, W.n, vset.p, voff.p,
                                                                         T.vert_tet);
+                D3G_TRY(async_pass(false, aleft2.p, anleft.p + 1, &nleft2));
+            }
+            async_left = nleft2;
+            // What the passes left goes through the rounds, maxw points at a time.
+            for (int off = 0; off < nleft2; off += maxw) {
+                W.n = std::min(maxw, nleft2 - off);
+                k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, aleft2.p + off, W.n, vset.p,
+                                                                        voff.p, T.vert_tet);
                 D3G_TRY(run_rounds());
             }
         } else {
             D3G_TRY(run_rounds());
         }
+        if (opt.validate) D3G_TRY(validate_tables("after", lev));
         if (trace) {
             cudaEventRecord(ev1, s);
             cudaEventSynchronize(ev1);
@@ -2237,19 +2664,21 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 won = (long long)ht1[0] - won_before;
                 attempts = (long long)ht1[1] - att_before;
             }
-            unsigned long long as[6] = {0, 0, 0, 0, 0, 0};
+            unsigned long long as[7] = {0, 0, 0, 0, 0, 0, 0};
             if (use_async) cudaMemcpy(as, astats.p, sizeof as, cudaMemcpyDeviceToHost);
             fprintf(stderr, "d3g level %d sets %zu workers %d rounds %d inserted %lld attempts %lld "
-                    "left-by-async %lld ms %.2f | async totals: lock-conflicts %llu walk-restarts %llu "
-                    "bad-seeds %llu too-big %llu left %llu first-left %llu\n",
-                    lev, descs.size(), W.n, round - round0, won, attempts, async_left, ms, as[0], as[1],
-                    as[2], as[3], as[4], as[5]);
+                    "left-by-fast-pass %lld left-by-async %lld ms %.2f | async totals: lock-conflicts %llu "
+                    "walk-restarts %llu bad-seeds %llu too-big %llu left %llu first-left %llu deferred %llu\n",
+                    lev, descs.size(), W.n, round - round0, won, attempts, deferred, async_left, ms, as[0],
+                    as[1], as[2], as[3], as[4], as[5], as[6]);
             cudaEventDestroy(ev0);
             cudaEventDestroy(ev1);
         }
     }
     {
-        unsigned long long hs2[2] = {0, 0}, ht[6], hst[2] = {0, 0};
+        unsigned long long hs2[2] = {0, 0}, ht[6], hst[2] = {0, 0}, hp[4] = {0, 0, 0, 0}, ha[7] = {};
+        D3G_CUDA(cudaMemcpyAsync(hp, pstats.p, sizeof hp, cudaMemcpyDeviceToHost, s));
+        if (use_async) D3G_CUDA(cudaMemcpyAsync(ha, astats.p, sizeof ha, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaMemcpyAsync(hs2, sums.p, sizeof hs2, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaMemcpyAsync(hst, steps.p, sizeof hst, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaMemcpyAsync(ht, totals.p, sizeof ht, cudaMemcpyDeviceToHost, s));
@@ -2260,6 +2689,11 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         R.stats.attempts = int64_t(ht[1]);
         R.stats.walk_steps = int64_t(hst[0]);
         R.stats.bfs_steps = int64_t(hst[1]);
+        R.stats.conflict_tests = int64_t(hp[0]);
+        R.stats.uncertain_tests = int64_t(hp[1]);
+        R.stats.tie_breaks = int64_t(hp[2]);
+        R.stats.max_region_tets = int64_t(hp[3]);
+        R.stats.deferred_points = int64_t(ha[6]);
     }
     // Release round scratch before the output stage.
     wcav.release();
@@ -2401,6 +2835,7 @@ void d3g_options_default(d3g_options* o) {
     o->tet_capacity = 0;
     o->walk_limit = 0;
     o->cavity_capacity = 0;
+    o->validate = 0;
     d3g_tuning t;
     if (current_tuning(&t)) {
         o->schedule = t.schedule;

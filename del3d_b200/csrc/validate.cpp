@@ -4,8 +4,11 @@
 // in range and at most one of them infinite; every triangular facet is shared
 // by exactly two cells, which induce opposite orientations on it (the complex
 // closes up and is consistently oriented, as the reference keeps it); and the
-// Euler characteristic V - E + F - T of the complex is 0, as for a
-// triangulated 3-sphere (the hull closed through the infinite vertex).  The
+// Euler characteristic V - E + F - T of the complex is 0.  These are necessary
+// conditions only: a triangulation of the points closed through the infinite
+// vertex is a 3-sphere and meets them, but so does any closed, consistently
+// oriented 3-manifold complex, and no geometry is looked at (a complex whose
+// orientation is flipped throughout, or that is not Delaunay, passes).  The
 // cells may come in any order and any even rotation.
 #include "../../include/del3d_b200.h"
 

@@ -182,6 +182,14 @@ typedef struct d3g_options {
                              /* normal scratch (256) and the big-round scratch   */
                              /* (16384), boundary facets at twice it; exceeded   */
                              /* in a big round: D3G_ERR_CAVITY_CAPACITY          */
+    int32_t validate;        /* debug: after each BRIO level, check the device   */
+                             /* tet table's invariants (the reference's          */
+                             /* Tds::validate(), src/tds.h:483-530): distinct    */
+                             /* vertices, live neighbours pointing back through  */
+                             /* the same facet, no lock left, every vertex's     */
+                             /* cached tet containing it; the first violation    */
+                             /* ends the build with D3G_ERR_INTERNAL and its     */
+                             /* description in d3g_last_error()                  */
 } d3g_options;
 
 /* What a build did (filled by d3g_build and d3g_build_device). */
@@ -199,8 +207,20 @@ typedef struct d3g_build_stats {
     int64_t walk_steps;      /* with timing: point-location steps over all attempts  */
     int64_t bfs_steps;       /* with timing: conflict-region growth steps (8 tets each) */
     double ms_async;         /* with timing: device time of the asynchronous passes  */
-    int64_t launches_async;  /* asynchronous passes (one per level)                  */
+    int64_t launches_async;  /* asynchronous passes (two per level: the fast variant */
+                             /* and the full one over what it deferred)              */
     int64_t async_inserted;  /* points the asynchronous passes inserted              */
+    /* Conflict tests (in_sphere, or orient3d against a hull facet) the insertion
+     * kernels evaluated, attempts that gave way included; of these, the ones the
+     * floating-point filter could not certify (decided by a set's exact filter
+     * value, the exact stage or a tie-break), and the ones whose exact value was
+     * zero (decided by the symbolic perturbation or the hull in-circle test). */
+    int64_t conflict_tests;
+    int64_t uncertain_tests;
+    int64_t tie_breaks;
+    int64_t max_region_tets;  /* the largest conflict region inserted (tets)         */
+    int64_t deferred_points;  /* points the fast asynchronous variant left to the    */
+                              /* full one (a test its filters could not decide)     */
 } d3g_build_stats;
 
 typedef struct d3g_result {
@@ -366,10 +386,12 @@ int d3g_microbench_fp64(int64_t iters, double* addmul_ops_per_s, double* fma_per
  * for all_cells() (infinite vertex = -1; any cell order, any even rotation): every
  * cell has four distinct vertices in [-1, n_points) (n_points <= 0: no upper bound)
  * with at most one infinite; every triangular facet is shared by exactly two cells
- * inducing opposite orientations on it; the Euler characteristic V - E + F - T is 0
- * (a triangulated 3-sphere: the hull closed through the infinite vertex).  Returns
- * D3G_OK, or D3G_ERR_INVALID_INPUT with the first violation in d3g_last_error().
- * No device is needed. */
+ * inducing opposite orientations on it; the Euler characteristic V - E + F - T is 0.
+ * Necessary conditions only (closed, consistently oriented, chi 0: a triangulation
+ * closed through the infinite vertex meets them, as does any closed oriented
+ * 3-manifold complex); no coordinates are read, so a complex flipped throughout or
+ * not Delaunay passes.  Returns D3G_OK, or D3G_ERR_INVALID_INPUT with the first
+ * violation in d3g_last_error().  No device is needed. */
 int d3g_validate_cells(const int32_t* all_cells, int64_t n_cells, int64_t n_points);
 
 /* ---- input readers (host) -------------------------------------------------------

@@ -97,3 +97,41 @@ def test_exact_capacity_build(cuda):
     d = d3.Delaunay()
     d.build(ok)
     assert np.array_equal(d.finite_cells(), oracle.canonical_cells(oracle.ref_build(ok)["cells"]))
+
+
+@pytest.mark.parametrize("dist", ["uniform", "clusters", "lattice", "sphere"])
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_validate_after_every_level(cuda, dist, schedule):
+    """The device port of the reference's Tds::validate() (src/tds.h:483-530),
+    run after every BRIO level, finds nothing wrong, and the cells are the same
+    as without it."""
+    import torch
+
+    pts = d3.gen_set(dist, 30_000, 41)
+    x = torch.from_numpy(pts).to(cuda)
+    stats = {}
+    a, nv = d3.build_device(x, schedule=schedule, validate=True, stats=stats)
+    a = a.clone()
+    b, nv2 = d3.build_device(x, schedule=schedule)
+    assert nv == nv2 and torch.equal(a, b)
+    # The per-build counters: every insertion made conflict tests; lattices need
+    # tie-breaks, uniform points none.
+    assert stats["conflict_tests"] > 10 * len(pts)
+    assert stats["max_region_tets"] >= 1
+    if dist == "lattice":
+        assert stats["tie_breaks"] > 0 and stats["uncertain_tests"] >= stats["tie_breaks"]
+    if dist == "uniform":
+        assert stats["tie_breaks"] == 0
+
+
+def test_validate_batched(cuda):
+    import torch
+
+    sets = d3.mixed_workload(64, 32, 8000, seed=5, first_seed=900)
+    offs = np.zeros(len(sets) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([len(a) for a in sets])
+    x = torch.from_numpy(np.concatenate(sets)).to(cuda)
+    a, co, nv = d3.build_batch_device(x, offs, validate=True)
+    a = a.clone()
+    b, co2, nv2 = d3.build_batch_device(x, offs)
+    assert (co == co2).all() and (nv == nv2).all() and torch.equal(a, b)
