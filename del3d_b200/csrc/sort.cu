@@ -547,11 +547,29 @@ __device__ int local_split(Local& L, int begin, int end, int axis, int up) {
     }
 }
 
+/// A node of the recursion inside a range of at most kSmall points, packed in
+/// 32 bits: begin and end (11 bits each), the axis (2 bits), the three
+/// directions (1 bit each).
+__device__ __forceinline__ uint32_t pack_node(int b, int e, int x, int ux, int uy, int uz) {
+    return uint32_t(b) | uint32_t(e) << 11 | uint32_t(x) << 22 | uint32_t(ux) << 24 | uint32_t(uy) << 25 |
+           uint32_t(uz) << 26;
+}
+
 /// One warp per range of at most kSmall points: the whole remaining recursion
-/// (spatial_sort.cpp:95-117) by lane 0 in shared memory.
+/// (spatial_sort.cpp:95-117) in shared memory.  The recursion's nodes cover
+/// disjoint index ranges and each one's splits read and permute only its own
+/// range, so once a node is split its eight children are independent of each
+/// other: the tree is processed level by level, the lanes taking the nodes of a
+/// level in turn, each node's seven splits done by one lane exactly as the
+/// reference does them.  The result is the reference's depth-first order, bit
+/// for bit.
 __global__ void __launch_bounds__(32) k_small_sort(const Seg* __restrict__ segs, Elems E) {
     __shared__ int32_t sidx[kSmall];
     __shared__ double sc[3][kSmall];
+    // Nodes of more than 8 points at one level: fewer than kSmall / 9 + 1.
+    constexpr int kNodes = kSmall / 9 + 1;
+    __shared__ uint32_t nodes[2][kNodes];
+    __shared__ int nnodes[2];
     const Seg g = segs[blockIdx.x];
     const int m = g.end - g.begin;
     for (int j = threadIdx.x; j < m; j += 32) {
@@ -560,35 +578,40 @@ __global__ void __launch_bounds__(32) k_small_sort(const Seg* __restrict__ segs,
         sc[1][j] = E.y[g.begin + j];
         sc[2][j] = E.z[g.begin + j];
     }
-    __syncwarp();
     if (threadIdx.x == 0) {
-        Local L{sidx, {sc[0], sc[1], sc[2]}};
-        Seg stack[64];
-        int top = 0;
-        stack[top++] = Seg{0, m, g.x, g.ux, g.uy, g.uz};
-        while (top > 0) {
-            const Seg f = stack[--top];
-            if (f.end - f.begin <= 8) continue;
-            const int x = f.x, y = (x + 1) % 3, z = (x + 2) % 3;
-            const int m0 = f.begin, m8 = f.end;
-            const int m4 = local_split(L, m0, m8, x, f.ux);
-            const int m2 = local_split(L, m0, m4, y, f.uy);
-            const int m1 = local_split(L, m0, m2, z, f.uz);
-            const int m3 = local_split(L, m2, m4, z, !f.uz);
-            const int m6 = local_split(L, m4, m8, y, !f.uy);
-            const int m5 = local_split(L, m4, m6, z, f.uz);
-            const int m7 = local_split(L, m6, m8, z, !f.uz);
-            stack[top++] = Seg{m0, m1, z, f.uz, f.ux, f.uy};
-            stack[top++] = Seg{m1, m2, y, f.uy, f.uz, f.ux};
-            stack[top++] = Seg{m2, m3, y, f.uy, f.uz, f.ux};
-            stack[top++] = Seg{m3, m4, x, f.ux, !f.uy, !f.uz};
-            stack[top++] = Seg{m4, m5, x, f.ux, !f.uy, !f.uz};
-            stack[top++] = Seg{m5, m6, y, !f.uy, f.uz, !f.ux};
-            stack[top++] = Seg{m6, m7, y, !f.uy, f.uz, !f.ux};
-            stack[top++] = Seg{m7, m8, z, !f.uz, !f.ux, f.uy};
-        }
+        nodes[0][0] = pack_node(0, m, g.x, g.ux, g.uy, g.uz);
+        nnodes[0] = m > 8 ? 1 : 0;
+        nnodes[1] = 0;
     }
     __syncwarp();
+    Local L{sidx, {sc[0], sc[1], sc[2]}};
+    for (int cur = 0; nnodes[cur] > 0; cur ^= 1) {
+        const int nxt = cur ^ 1;
+        const int count = nnodes[cur];
+        for (int k = threadIdx.x; k < count; k += 32) {
+            const uint32_t f = nodes[cur][k];
+            const int m0 = int(f & 0x7FFu), m8 = int((f >> 11) & 0x7FFu), x = int((f >> 22) & 3u);
+            const int ux = int((f >> 24) & 1u), uy = int((f >> 25) & 1u), uz = int((f >> 26) & 1u);
+            const int y = (x + 1) % 3, z = (x + 2) % 3;
+            const int m4 = local_split(L, m0, m8, x, ux);
+            const int m2 = local_split(L, m0, m4, y, uy);
+            const int m1 = local_split(L, m0, m2, z, uz);
+            const int m3 = local_split(L, m2, m4, z, !uz);
+            const int m6 = local_split(L, m4, m8, y, !uy);
+            const int m5 = local_split(L, m4, m6, z, uz);
+            const int m7 = local_split(L, m6, m8, z, !uz);
+            const uint32_t ch[8] = {pack_node(m0, m1, z, uz, ux, uy),   pack_node(m1, m2, y, uy, uz, ux),
+                                    pack_node(m2, m3, y, uy, uz, ux),   pack_node(m3, m4, x, ux, !uy, !uz),
+                                    pack_node(m4, m5, x, ux, !uy, !uz), pack_node(m5, m6, y, !uy, uz, !ux),
+                                    pack_node(m6, m7, y, !uy, uz, !ux), pack_node(m7, m8, z, !uz, !ux, uy)};
+            const int lo[8] = {m0, m1, m2, m3, m4, m5, m6, m7}, hi[8] = {m1, m2, m3, m4, m5, m6, m7, m8};
+            for (int c = 0; c < 8; ++c)
+                if (hi[c] - lo[c] > 8) nodes[nxt][atomicAdd(&nnodes[nxt], 1)] = ch[c];
+        }
+        __syncwarp();
+        if (threadIdx.x == 0) nnodes[cur] = 0;
+        __syncwarp();
+    }
     for (int j = threadIdx.x; j < m; j += 32) E.idx[g.begin + j] = sidx[j];
 }
 
