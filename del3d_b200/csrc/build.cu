@@ -735,7 +735,11 @@ struct AsyncCtx {
     int* next;                      // chunk queue head
     int* leftover;                  // points left for the rounds
     int* n_leftover;
-    int64_t stride;                 // chunk q of the queue is chunk (q * stride) % W.n
+    int64_t stride;                 // entry q of the queue is worker (q * stride) % nw ...
+    const int* wlist;               // ... of this list (null: of all W.n workers)
+    int nw;
+    int* passed;                    // kFast: workers passed on whole to the full variant
+    int* n_passed;
     unsigned long long* ekey;       // per warp slot: 3 edge keys per boundary facet (re-star)
     unsigned long long* stats;      // [0] lock conflicts, [1] walk restarts, [2] invalid seeds,
                                     // [3] regions too big, [4] points left, [5] first points left,
@@ -1262,11 +1266,20 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
         int q = 0;
         if (lane == 0) q = atomicAdd(A.next, 1);
         q = __shfl_sync(kFull, q, 0);
-        if (q >= W.n) break;
-        const int w = int((int64_t(q) * A.stride) % W.n);
+        if (q >= A.nw) break;
+        const int wq = int((int64_t(q) * A.stride) % A.nw);
+        const int w = A.wlist ? A.wlist[wq] : wq;
+        const bool ex = W.set_exact[W.wset[w]] != 0;
+        if (kFast && ex) {
+            // A set whose coordinates make the filters exact (integer lattices,
+            // coarse grids) needs the hull in-circle test wherever points lie in
+            // the planes of hull facets - much of the time: its chunks go whole
+            // to the full variant.
+            if (lane == 0) A.passed[atomicAdd(A.n_passed, 1)] = w;
+            continue;
+        }
         const int b = W.beg[w], len = W.end[w] - b;
         const int4 sk = W.skips[W.wset[w]];
-        const bool ex = W.set_exact[W.wset[w]] != 0;
         int pos = W.pos[w], left = W.left[w];
         int v = W.cur[w];
         int last = -1;
@@ -2339,7 +2352,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     // the full variant over what that leaves; the rounds finish the rest.
     const bool use_async = opt.schedule != 1 && !grow;
     constexpr int kAsyncWarps = kNumSMs * 32;   // resident at 64 registers a thread
-    DevBuf<int> alock, anext, aleft, aleft2, anleft;
+    DevBuf<int> alock, anext, aleft, aleft2, anleft, apassed;
     DevBuf<unsigned long long> astats, aekey;
     if (use_async) {
         D3G_TRY(aekey.alloc(size_t(std::min(maxw, kAsyncWarps)) * 3 * size_t(W.fac_cap), s));
@@ -2347,7 +2360,8 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         D3G_TRY(anext.alloc(1, s));
         D3G_TRY(aleft.alloc(size_t(nv), s));
         D3G_TRY(aleft2.alloc(size_t(nv), s));
-        D3G_TRY(anleft.alloc(2, s));
+        D3G_TRY(anleft.alloc(3, s));
+        D3G_TRY(apassed.alloc(size_t(maxw), s));
         D3G_TRY(astats.alloc(7, s));
         D3G_CUDA(cudaMemsetAsync(alock.p, 0, sizeof(int) * size_t(T.cap), s));
         D3G_CUDA(cudaMemsetAsync(astats.p, 0, 7 * sizeof(unsigned long long), s));
@@ -2590,15 +2604,17 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             // One asynchronous pass: a persistent grid over the workers W
             // (level chunks, or one leftover point each), writing the points it
             // leaves to `left` / `nleft_d`; their count goes to *nleft_out.
-            auto async_pass = [&](bool fast, int* left, int* nleft_d, int* nleft_out) -> int {
+            auto async_pass = [&](bool fast, const int* wlist, int nw, int* left, int* nleft_d,
+                                  int* nleft_out) -> int {
                 // The chunks go out in a scattered order (stride coprime with the
                 // chunk count, near the golden ratio of it), so that chunks taken
                 // at the same time lie far apart along the curve.
-                int64_t stride = std::max<int64_t>(1, int64_t(double(W.n) * 0.6180339887));
-                while (std::gcd(stride, int64_t(W.n)) != 1) ++stride;
+                int64_t stride = std::max<int64_t>(1, int64_t(double(nw) * 0.6180339887));
+                while (std::gcd(stride, int64_t(nw)) != 1) ++stride;
                 D3G_CUDA(cudaMemsetAsync(anext.p, 0, sizeof(int), s));
-                AsyncCtx A{alock.p, anext.p, left, nleft_d, stride, aekey.p, astats.p};
-                const int warps = std::min(W.n, kAsyncWarps);
+                AsyncCtx A{alock.p, anext.p, left, nleft_d, stride, wlist, nw, apassed.p, anleft.p + 2, aekey.p,
+                           astats.p};
+                const int warps = std::min(nw, kAsyncWarps);
                 const unsigned grid = unsigned((int64_t(warps) * 32 + 127) / 128);
                 unsigned long long won0 = 0;
                 D3G_CUDA(cudaMemcpyAsync(&won0, totals.p, sizeof won0, cudaMemcpyDeviceToHost, s));
@@ -2627,19 +2643,23 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 }
                 return D3G_OK;
             };
-            // The level's chunks through the fast variant; what it deferred or
-            // left (undecided tests, lock conflicts, regions too big) through
-            // the full variant, one worker per point, maxw points at a time;
-            // what that leaves through the rounds.
-            int nleft = 0, nleft2 = 0;
-            D3G_CUDA(cudaMemsetAsync(anleft.p, 0, 2 * sizeof(int), s));
-            D3G_TRY(async_pass(true, aleft.p, anleft.p, &nleft));
+            // The level's chunks through the fast variant, the chunks of sets
+            // whose filters are exact through the full variant; what they
+            // deferred or left (undecided tests, lock conflicts, regions too
+            // big) through the full variant, one worker per point, maxw points
+            // at a time; what that leaves through the rounds.
+            int nleft = 0, nleft2 = 0, npassed = 0;
+            D3G_CUDA(cudaMemsetAsync(anleft.p, 0, 3 * sizeof(int), s));
+            D3G_TRY(async_pass(true, nullptr, W.n, aleft.p, anleft.p, &nleft));
+            D3G_CUDA(cudaMemcpyAsync(&npassed, anleft.p + 2, sizeof npassed, cudaMemcpyDeviceToHost, s));
+            D3G_CUDA(cudaStreamSynchronize(s));
+            if (npassed > 0) D3G_TRY(async_pass(false, apassed.p, npassed, aleft.p, anleft.p, &nleft));
             deferred = nleft;
             for (int off = 0; off < nleft; off += maxw) {
                 W.n = std::min(maxw, nleft - off);
                 k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, aleft.p + off, W.n, vset.p, voff.p,
                                                                         T.vert_tet);
-                D3G_TRY(async_pass(false, aleft2.p, anleft.p + 1, &nleft2));
+                D3G_TRY(async_pass(false, nullptr, W.n, aleft2.p, anleft.p + 1, &nleft2));
             }
             async_left = nleft2;
             // What the passes left goes through the rounds, maxw points at a time.

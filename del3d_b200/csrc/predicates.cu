@@ -11,6 +11,7 @@
 // The coplanar family, used only on hull-coplanar configurations, runs as one
 // kernel per query.
 #include "common.cuh"
+#include "exact_wide.cuh"
 
 #include <cuda.h>
 
@@ -18,6 +19,12 @@
 
 namespace d3g {
 namespace {
+
+// The wide tier: at most this many calls queued per entry-point call (more
+// report D3G_ERR_EXACT_CAPACITY), and this many evaluated at once (each with a
+// kWideArenaLimbs piece of the arena: 148 KB).
+constexpr int64_t kWideQueueCap = int64_t(1) << 20;
+constexpr int64_t kWideSlots = 256;
 
 __device__ __forceinline__ Pt load_pt(const double* __restrict__ pts, int32_t i) {
     const double* p = pts + 3 * int64_t(i);
@@ -36,6 +43,36 @@ __device__ __forceinline__ void warp_push(bool push, int64_t q, int64_t* queue,
     if (lane == __ffs(mask) - 1) base = atomicAdd(count, (unsigned long long)__popc(mask));
     base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
     if (push) queue[base + __popc(mask & ((1u << lane) - 1u))] = q;
+}
+
+/// Limbs the exact stage needs for an orient3d / in_sphere call (0 when the
+/// filter's own value is exact), as orient3d_degenerate / in_sphere_degenerate
+/// choose them.
+__device__ int orient3d_limbs(const Pt& a, const Pt& b, const Pt& c, const Pt& d) {
+    Span s;
+    s.add(a.x); s.add(a.y); s.add(a.z); s.add(b.x); s.add(b.y); s.add(b.z);
+    s.add(c.x); s.add(c.y); s.add(c.z); s.add(d.x); s.add(d.y); s.add(d.z);
+    return s.exact_in_double(3, 3) ? 0 : limbs_for(3 * (s.bits() + 1) + 3);
+}
+__device__ int in_sphere_limbs(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e) {
+    Span s;
+    s.add(a.x); s.add(a.y); s.add(a.z); s.add(b.x); s.add(b.y); s.add(b.z);
+    s.add(c.x); s.add(c.y); s.add(c.z); s.add(d.x); s.add(d.y); s.add(d.z);
+    s.add(e.x); s.add(e.y); s.add(e.z);
+    return s.exact_in_double(5, 7) ? 0 : limbs_for(5 * (s.bits() + 1) + 7);
+}
+
+/// Queues query q for the wide tier (too wide for the exact stage's 16 limbs),
+/// or reports the exact-stage capacity when the caller gave no wide queue (the
+/// entry point that allocates nothing) or it is full.
+__device__ void push_wide(int64_t q, int64_t* wq, unsigned long long* wcount, int64_t wcap, uint32_t* status) {
+    if (!wq) {
+        report(status, ST_EXACT_CAPACITY);
+        return;
+    }
+    const unsigned long long k = atomicAdd(wcount, 1ull);
+    if (int64_t(k) < wcap) wq[k] = q;
+    else report(status, ST_EXACT_CAPACITY);
 }
 
 __global__ void __launch_bounds__(256) k_filter_orient3d(const double* __restrict__ pts, int64_t npts,
@@ -67,6 +104,7 @@ __global__ void __launch_bounds__(256) k_exact_orient3d(const double* __restrict
                                                         int8_t* __restrict__ out,
                                                         const int64_t* __restrict__ queue,
                                                         const unsigned long long* qcount,
+                                                        int64_t* wq, unsigned long long* wcount, int64_t wcap,
                                                         uint32_t* status) {
     const int64_t n = int64_t(*qcount);
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
@@ -75,6 +113,10 @@ __global__ void __launch_bounds__(256) k_exact_orient3d(const double* __restrict
         const int4 t = *reinterpret_cast<const int4*>(idx + 4 * q);
         const Pt a = load_pt(pts, t.x), b = load_pt(pts, t.y), c = load_pt(pts, t.z),
                  d = load_pt(pts, t.w);
+        if (orient3d_limbs(a, b, c, d) > kMaxLimbs) {
+            push_wide(q, wq, wcount, wcap, status);
+            continue;
+        }
         const Orient3dFilter f = orient3d_filter(a, b, c, d);
         out[q] = int8_t(orient3d_exact(a, b, c, d, f.det, status));
     }
@@ -112,7 +154,9 @@ __global__ void __launch_bounds__(128) k_exact_in_sphere(const double* __restric
                                                          int8_t* __restrict__ out,
                                                          const int64_t* __restrict__ queue,
                                                          const unsigned long long* qcount,
-                                                         int perturbed, uint32_t* status) {
+                                                         int perturbed, int64_t* wq,
+                                                         unsigned long long* wcount, int64_t wcap,
+                                                         uint32_t* status) {
     const int64_t n = int64_t(*qcount);
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
          k += int64_t(gridDim.x) * blockDim.x) {
@@ -121,11 +165,84 @@ __global__ void __launch_bounds__(128) k_exact_in_sphere(const double* __restric
         const int64_t id[5] = {t[0], t[1], t[2], t[3], t[4]};
         const Pt a = load_pt(pts, t[0]), b = load_pt(pts, t[1]), c = load_pt(pts, t[2]),
                  d = load_pt(pts, t[3]), e = load_pt(pts, t[4]);
+        // Too wide for 16 limbs: the wide tier (a tie-break then needs orient3d
+        // calls of at most this width, so narrower calls never get there).
+        if (in_sphere_limbs(a, b, c, d, e) > kMaxLimbs) {
+            push_wide(q, wq, wcount, wcap, status);
+            continue;
+        }
         const InSphereFilter f = in_sphere_filter(a, b, c, d, e);
         const int s = in_sphere_degenerate(a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z, d.x, d.y, d.z, e.x, e.y,
                                            e.z, id[0], id[1], id[2], id[3], id[4], f.det, perturbed, status);
         out[q] = int8_t(s);
     }
+}
+
+// ---- the wide tier ------------------------------------------------------------
+//
+// Calls whose exact value needs more than the exact stage's 16 limbs (coordinate
+// spans beyond about 200 binades in one in_sphere call, 330 in one orient3d
+// call).  One thread per call, its integers in its own piece of an arena the
+// host allocates for the calls queued (exact_wide.cuh); rare and slow by design,
+// but every finite input gets the reference's sign.
+
+/// orient3d for the tie-break of a wide in_sphere call: the filter, then the
+/// exact stage's tiers, then the arena when 16 limbs are not enough.
+struct Orient3dWide {
+    Arena* arena;
+    uint32_t* status;
+    __device__ int operator()(const Pt& A, const Pt& B, const Pt& C, const Pt& D) const {
+        const Orient3dFilter f = orient3d_filter(A, B, C, D);
+        if (f.certain) return -sign_of(f.det);
+        const int L = orient3d_limbs(A, B, C, D);
+        if (L <= kMaxLimbs) return orient3d_exact(A, B, C, D, f.det, status);
+        Span s;
+        s.add(A.x); s.add(A.y); s.add(A.z); s.add(B.x); s.add(B.y); s.add(B.z);
+        s.add(C.x); s.add(C.y); s.add(C.z); s.add(D.x); s.add(D.y); s.add(D.z);
+        const int64_t mark = arena->used;
+        const int r = orient3d_num<WideG>(A, B, C, D, NumFrom<WideG>{s.emin, L, arena});
+        if (!arena->overflow) arena->used = mark;
+        return r;
+    }
+};
+
+__global__ void __launch_bounds__(64) k_wide_orient3d(const double* __restrict__ pts, const int32_t* __restrict__ idx,
+                                                      int8_t* __restrict__ out, const int64_t* __restrict__ wq,
+                                                      int64_t first, int64_t count, uint64_t* arena,
+                                                      int64_t arena_limbs, uint32_t* status) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int64_t q = wq[first + k];
+    const int4 t = *reinterpret_cast<const int4*>(idx + 4 * q);
+    Arena A{arena + k * arena_limbs, arena_limbs, 0, false};
+    const int s = Orient3dWide{&A, status}(load_pt(pts, t.x), load_pt(pts, t.y), load_pt(pts, t.z),
+                                           load_pt(pts, t.w));
+    if (A.overflow) report(status, ST_EXACT_CAPACITY);
+    out[q] = int8_t(s);
+}
+
+__global__ void __launch_bounds__(64) k_wide_in_sphere(const double* __restrict__ pts, const int32_t* __restrict__ idx,
+                                                       int8_t* __restrict__ out, const int64_t* __restrict__ wq,
+                                                       int64_t first, int64_t count, int perturbed, uint64_t* arena,
+                                                       int64_t arena_limbs, uint32_t* status) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int64_t q = wq[first + k];
+    const int32_t* t = idx + 5 * q;
+    const Pt a = load_pt(pts, t[0]), b = load_pt(pts, t[1]), c = load_pt(pts, t[2]), d = load_pt(pts, t[3]),
+             e = load_pt(pts, t[4]);
+    Arena A{arena + k * arena_limbs, arena_limbs, 0, false};
+    Span s;
+    s.add(a.x); s.add(a.y); s.add(a.z); s.add(b.x); s.add(b.y); s.add(b.z);
+    s.add(c.x); s.add(c.y); s.add(c.z); s.add(d.x); s.add(d.y); s.add(d.z);
+    s.add(e.x); s.add(e.y); s.add(e.z);
+    const int L = limbs_for(5 * (s.bits() + 1) + 7);
+    int sign = in_sphere_num<WideG>(a, b, c, d, e, NumFrom<WideG>{s.emin, L, &A});
+    if (!A.overflow) A.used = 0;
+    if (sign == 0 && perturbed)
+        sign = in_sphere_perturb_by(Orient3dWide{&A, status}, a, b, c, d, e, t[0], t[1], t[2], t[3], t[4]);
+    if (A.overflow) report(status, ST_EXACT_CAPACITY);
+    out[q] = int8_t(sign);
 }
 
 __global__ void __launch_bounds__(128) k_coplanar(const double* __restrict__ pts, int64_t npts,
@@ -198,39 +315,68 @@ int predicates_device(const double* d_pts, int64_t n_pts, const int32_t* d_idx, 
         set_error("d3g_predicates: orient3d index array must be 16-byte aligned");
         return D3G_ERR_INVALID_ARGUMENT;
     }
-    // Scratch: status word, queue counter, and the exact-stage queue.
+    // Scratch: status word, queue counter, wide-queue counter, and the queues
+    // of the exact stage and of its wide tier.
     DevBuf<unsigned long long> counters;
-    D3G_TRY(counters.alloc(2, stream));
-    D3G_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(unsigned long long), stream));
+    D3G_TRY(counters.alloc(3, stream));
+    D3G_CUDA(cudaMemsetAsync(counters.p, 0, 3 * sizeof(unsigned long long), stream));
     uint32_t* status = reinterpret_cast<uint32_t*>(counters.p);
     unsigned long long* qcount = counters.p + 1;
-    DevBuf<int64_t> queue;
+    unsigned long long* wcount = counters.p + 2;
+    DevBuf<int64_t> queue, wqueue;
+    const int64_t wcap = std::min<int64_t>(nq, kWideQueueCap);
     const int blk = 256;
-    if (kind == D3G_ORIENT3D || kind == D3G_IN_SPHERE || kind == D3G_IN_SPHERE_UNPERTURBED) {
+    const bool queued = kind == D3G_ORIENT3D || kind == D3G_IN_SPHERE || kind == D3G_IN_SPHERE_UNPERTURBED;
+    if (queued) {
         D3G_TRY(queue.alloc(size_t(nq), stream));
+        D3G_TRY(wqueue.alloc(size_t(wcap), stream));
         const unsigned g = grid_for(nq, blk, int64_t(kNumSMs) * 16);
         if (kind == D3G_ORIENT3D) {
             k_filter_orient3d<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, queue.p, qcount,
                                                      status);
-            k_exact_orient3d<<<kNumSMs * 4, 256, 0, stream>>>(d_pts, d_idx, d_out, queue.p, qcount,
-                                                             status);
+            k_exact_orient3d<<<kNumSMs * 4, 256, 0, stream>>>(d_pts, d_idx, d_out, queue.p, qcount, wqueue.p,
+                                                             wcount, wcap, status);
         } else {
             k_filter_in_sphere<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, queue.p,
                                                       qcount, status);
-            k_exact_in_sphere<<<kNumSMs * 8, 128, 0, stream>>>(
-                d_pts, d_idx, d_out, queue.p, qcount, kind == D3G_IN_SPHERE ? 1 : 0, status);
+            k_exact_in_sphere<<<kNumSMs * 8, 128, 0, stream>>>(d_pts, d_idx, d_out, queue.p, qcount,
+                                                               kind == D3G_IN_SPHERE ? 1 : 0, wqueue.p, wcount,
+                                                               wcap, status);
         }
     } else {
         k_coplanar<<<grid_for(nq, 128), 128, 0, stream>>>(d_pts, n_pts, d_idx, nq, kind, d_out,
                                                           qcount, status);
     }
     D3G_CUDA(cudaGetLastError());
-    unsigned long long host_counters[2] = {0, 0};
+    unsigned long long host_counters[3] = {0, 0, 0};
     D3G_CUDA(cudaMemcpyAsync(host_counters, counters.p, sizeof host_counters, cudaMemcpyDeviceToHost,
                              stream));
     queue.release();
-    counters.release();
     D3G_CUDA(cudaStreamSynchronize(stream));
+    // The wide tier, for the calls queued: kWideSlots at a time, each thread
+    // with its own piece of the arena.
+    const int64_t nwide = std::min<int64_t>(int64_t(host_counters[2]), wcap);
+    if (queued && nwide > 0 && (uint32_t(host_counters[0]) & ST_INTERNAL) == 0) {
+        DevBuf<uint64_t> arena;
+        const int64_t slots = std::min<int64_t>(nwide, kWideSlots);
+        D3G_TRY(arena.alloc(size_t(slots) * size_t(kWideArenaLimbs), stream));
+        for (int64_t first = 0; first < nwide; first += slots) {
+            const int64_t cnt = std::min<int64_t>(slots, nwide - first);
+            if (kind == D3G_ORIENT3D)
+                k_wide_orient3d<<<unsigned((cnt + 63) / 64), 64, 0, stream>>>(d_pts, d_idx, d_out, wqueue.p, first,
+                                                                           cnt, arena.p, kWideArenaLimbs, status);
+            else
+                k_wide_in_sphere<<<unsigned((cnt + 63) / 64), 64, 0, stream>>>(
+                    d_pts, d_idx, d_out, wqueue.p, first, cnt, kind == D3G_IN_SPHERE ? 1 : 0, arena.p,
+                    kWideArenaLimbs, status);
+            D3G_CUDA(cudaGetLastError());
+        }
+        D3G_CUDA(cudaMemcpyAsync(host_counters, counters.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 stream));
+        D3G_CUDA(cudaStreamSynchronize(stream));
+    }
+    wqueue.release();
+    counters.release();
     if (stats) *stats = d3g_predicate_stats{nq, int64_t(host_counters[1])};
     const uint32_t bits = uint32_t(host_counters[0]);
     if (bits & ST_INTERNAL) {
@@ -377,12 +523,13 @@ int predicates_noalloc_device(const double* d_pts, int64_t n_pts, const int32_t*
             k_filter_orient3d<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, sc->queue, qcount,
                                                      status);
             k_exact_orient3d<<<kNumSMs * 4, 256, 0, stream>>>(d_pts, d_idx, d_out, sc->queue, qcount,
-                                                             status);
+                                                             nullptr, nullptr, 0, status);
         } else {
             k_filter_in_sphere<<<g, blk, 0, stream>>>(d_pts, n_pts, d_idx, nq, d_out, sc->queue,
                                                       qcount, status);
             k_exact_in_sphere<<<kNumSMs * 8, 128, 0, stream>>>(
-                d_pts, d_idx, d_out, sc->queue, qcount, kind == D3G_IN_SPHERE ? 1 : 0, status);
+                d_pts, d_idx, d_out, sc->queue, qcount, kind == D3G_IN_SPHERE ? 1 : 0, nullptr, nullptr, 0,
+                status);
         }
     } else {
         k_coplanar<<<grid_for(nq, 128), 128, 0, stream>>>(d_pts, n_pts, d_idx, nq, kind, d_out,

@@ -321,9 +321,9 @@ D3G_HD int lexico_last(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const
 /// gives NEGATIVE; the first other point whose replacement by e gives a
 /// non-zero orient3d gives that sign.  `id0..id4` are the identities of a..e
 /// (the reference compares pointers, so equal identities are the same point).
-template <bool EX = false>
-D3G_HD int in_sphere_perturb(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e, int64_t id0,
-                             int64_t id1, int64_t id2, int64_t id3, int64_t id4, uint32_t* status) {
+template <class Orient>
+D3G_HD int in_sphere_perturb_by(const Orient& orient, const Pt& a, const Pt& b, const Pt& c, const Pt& d,
+                                const Pt& e, int64_t id0, int64_t id1, int64_t id2, int64_t id3, int64_t id4) {
     int skip = -1;
 #pragma unroll 1
     for (int r = 0; r < 2; ++r) {
@@ -340,11 +340,26 @@ D3G_HD int in_sphere_perturb(const Pt& a, const Pt& b, const Pt& c, const Pt& d,
             const Pt& B = j == 1 ? e : b;
             const Pt& C = j == 2 ? e : c;
             const Pt& D = j == 3 ? e : d;
-            const int o = orient3d_x(A, B, C, D, EX, status);
+            const int o = orient(A, B, C, D);
             if (o != 0) return o;
         }
     }
     return -1;
+}
+
+/// orient3d_x as a function object (the orientation the tie-break uses).
+template <bool EX>
+struct Orient3dX {
+    uint32_t* status;
+    D3G_HD int operator()(const Pt& A, const Pt& B, const Pt& C, const Pt& D) const {
+        return orient3d_x(A, B, C, D, EX, status);
+    }
+};
+
+template <bool EX = false>
+D3G_HD int in_sphere_perturb(const Pt& a, const Pt& b, const Pt& c, const Pt& d, const Pt& e, int64_t id0,
+                             int64_t id1, int64_t id2, int64_t id3, int64_t id4, uint32_t* status) {
+    return in_sphere_perturb_by(Orient3dX<EX>{status}, a, b, c, d, e, id0, id1, id2, id3, id4);
 }
 
 /// Exact sign of in_sphere (and, with `perturbed`, the tie-break) for a call the

@@ -78,16 +78,32 @@ def _wide_octahedron(k):
     return pts
 
 
-def test_exact_capacity_predicate(cuda):
-    # 250 binades in one in_sphere call need more than the exact stage's 16
-    # limbs: a status, not a sign.  At 200 binades the sign is the reference's.
+def test_wide_exact_tier_predicates(cuda):
+    """Calls whose exact value needs more than the exact stage's 16 limbs (in_sphere
+    over more than about 200 binades, orient3d over more than about 330) go to the
+    wide tier and get the reference's sign: the octahedron moved off its sphere by
+    2^-k up to k = 1070, and random points with exponents over the whole double
+    range, against the reference's predicates and its integer oracle."""
     idx = np.array([[0, 1, 2, 3, 4]], np.int32)
-    ok = _wide_octahedron(200)
-    assert (d3.in_sphere(ok, idx) == oracle.ref_predicate("in_sphere", ok, idx)).all()
-    with pytest.raises(d3.Del3dError) as e:
-        d3.in_sphere(_wide_octahedron(250), idx)
-    assert e.value.status == d3.ERR_EXACT_CAPACITY
-    assert (d3.in_sphere(ok, idx) == oracle.ref_predicate("in_sphere", ok, idx)).all()
+    for k in list(range(200, 1071, 29)) + [1074]:
+        pts = _wide_octahedron(k)
+        for kind, fn in (("in_sphere", d3.in_sphere), ("in_sphere_unperturbed", d3.in_sphere_unperturbed)):
+            got = fn(pts, idx)
+            assert (got == oracle.ref_predicate(kind, pts, idx)).all(), (kind, k)
+            assert (got == oracle.exact_predicate(kind, pts, idx)).all(), (kind, k)
+    rng = np.random.default_rng(31)
+    pts = rng.uniform(-1, 1, (3000, 3)) * 2.0 ** rng.integers(-1000, 1000, (3000, 1))
+    pts[::7, 1] = 0.0
+    q = rng.integers(0, len(pts), (20000, 5)).astype(np.int32)
+    for kind, fn, ii in (("orient3d", d3.orient3d, q[:, :4]), ("in_sphere", d3.in_sphere, q),
+                         ("in_sphere_unperturbed", d3.in_sphere_unperturbed, q)):
+        got = fn(pts, ii)
+        assert (got == oracle.ref_predicate(kind, pts, ii)).all(), kind
+    # Points on a plane through the origin tilted by 2^-800: orient3d exactly
+    # resolvable only with about 2400 bits.
+    plane = np.array([[1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0], [2.0 ** -800, 0.5, 0.5]])
+    o = np.array([[0, 1, 2, 3], [1, 0, 2, 3]], np.int32)
+    assert (d3.orient3d(plane, o) == oracle.exact_predicate("orient3d", plane, o)).all()
 
 
 def test_exact_capacity_build(cuda):

@@ -107,13 +107,31 @@ def test_noalloc_at_the_limit_matches_counts(cuda):
     idx = torch.from_numpy(idx_h).to(cuda)
     res = {}
     for name in ("d3g_predicates_noalloc_device", "d3g_predicates_device"):
-        st = (ctypes.c_int64 * 2)()
+        st = d3._PredStats()
         out = torch.zeros(MAX_QUERIES, dtype=torch.int8, device=cuda)
         rc = getattr(lib, name)(pts.data_ptr(), pts.shape[0], idx.data_ptr(), MAX_QUERIES, d3.IN_SPHERE,
-                                out.data_ptr(), None, ctypes.cast(st, ctypes.c_void_p))
+                                out.data_ptr(), None, ctypes.byref(st))
         assert rc == 0, lib.d3g_last_error().decode()
-        res[name] = (out.cpu().numpy(), st[0], st[1])
+        res[name] = (out.cpu().numpy(), st.n_queries, st.n_exact)
     got, want = res["d3g_predicates_noalloc_device"], res["d3g_predicates_device"]
     assert got[1] == want[1] == MAX_QUERIES
     assert got[2] == want[2] == MAX_QUERIES, (got[2], want[2])
     assert np.array_equal(got[0], want[0])
+
+
+def test_noalloc_reports_calls_beyond_the_exact_stage(cuda):
+    """The fixed array holds no arena for the wide tier: an in_sphere call whose
+    exact value needs more than 16 limbs is reported (D3G_ERR_EXACT_CAPACITY),
+    never answered wrongly; the allocating entry point answers it."""
+    import torch
+
+    lib = _lib()
+    pts_h = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [-1, 0, 0], [2.0 ** -250, 0, -1]], dtype=np.float64)
+    pts = torch.from_numpy(pts_h).to(cuda)
+    idx = torch.tensor([[0, 1, 2, 3, 4]], dtype=torch.int32, device=cuda)
+    out = torch.zeros(1, dtype=torch.int8, device=cuda)
+    st = lib.d3g_predicates_noalloc_device(pts.data_ptr(), 5, idx.data_ptr(), 1, d3.IN_SPHERE, out.data_ptr(),
+                                           None, None)
+    assert st == d3.ERR_EXACT_CAPACITY
+    assert _run(lib.d3g_predicates_device, pts, idx, d3.IN_SPHERE, torch)[0] == \
+        oracle.ref_predicate("in_sphere", pts_h, np.array([[0, 1, 2, 3, 4]], np.int32))[0]
