@@ -81,24 +81,59 @@ def _wide_octahedron(k):
 def test_wide_exact_tier_predicates(cuda):
     """Calls whose exact value needs more than the exact stage's 16 limbs (in_sphere
     over more than about 200 binades, orient3d over more than about 330) go to the
-    wide tier and get the reference's sign: the octahedron moved off its sphere by
-    2^-k up to k = 1070, and random points with exponents over the whole double
-    range, against the reference's predicates and its integer oracle."""
+    wide tier and get the exact sign: the octahedron moved off its sphere by 2^-k
+    up to k = 1074, and random points with exponents over wide ranges, against the
+    reference's integer oracle tests/exact.h, and against the reference's own
+    predicates wherever its floating-point expansions cannot underflow or overflow.
+    (Where they do - products of coordinates below 2^-1074, e.g. the octahedron
+    moved by 2^-548 or less - the reference's sign is not the exact one; this
+    library's is.)"""
     idx = np.array([[0, 1, 2, 3, 4]], np.int32)
     for k in list(range(200, 1071, 29)) + [1074]:
         pts = _wide_octahedron(k)
         for kind, fn in (("in_sphere", d3.in_sphere), ("in_sphere_unperturbed", d3.in_sphere_unperturbed)):
             got = fn(pts, idx)
-            assert (got == oracle.ref_predicate(kind, pts, idx)).all(), (kind, k)
             assert (got == oracle.exact_predicate(kind, pts, idx)).all(), (kind, k)
+            if 2 * k <= 1074:
+                assert (got == oracle.ref_predicate(kind, pts, idx)).all(), (kind, k)
     rng = np.random.default_rng(31)
-    pts = rng.uniform(-1, 1, (3000, 3)) * 2.0 ** rng.integers(-1000, 1000, (3000, 1))
+    # Exponents in [-200, 200]: spans of up to 400 binades, no under/overflow in
+    # the reference's degree-5 expansions.
+    pts = rng.uniform(-1, 1, (3000, 3)) * 2.0 ** rng.integers(-200, 200, (3000, 1))
     pts[::7, 1] = 0.0
     q = rng.integers(0, len(pts), (20000, 5)).astype(np.int32)
     for kind, fn, ii in (("orient3d", d3.orient3d, q[:, :4]), ("in_sphere", d3.in_sphere, q),
                          ("in_sphere_unperturbed", d3.in_sphere_unperturbed, q)):
         got = fn(pts, ii)
         assert (got == oracle.ref_predicate(kind, pts, ii)).all(), kind
+        assert (got[:2000] == oracle.exact_predicate(kind, pts, ii[:2000])).all(), kind
+    # The whole double range (the exact oracle is slow here: a few hundred calls).
+    wide = rng.uniform(-1, 1, (400, 3)) * 2.0 ** rng.integers(-1070, 1000, (400, 1))
+    qw = rng.integers(0, len(wide), (300, 5)).astype(np.int32)
+    for kind, fn, ii in (("orient3d", d3.orient3d, qw[:, :4]), ("in_sphere", d3.in_sphere, qw)):
+        assert (fn(wide, ii) == oracle.exact_predicate(kind, wide, ii)).all(), kind
+    # Nearly cospherical calls that need the wide tier: five points of an integer
+    # lattice sphere (squared radius 1105^2) scaled by 2^s, the fifth moved by
+    # 2^(s-300) - every call uncertain for the filter, spanning about 310 binades.
+    from bench import lattice_sphere_vectors
+
+    vecs = lattice_sphere_vectors(1105 * 1105).astype(np.float64)
+    with_zero = vecs[(vecs == 0).any(axis=1)]
+    groups = []
+    for g in range(200):
+        sc = float(rng.integers(100, 190))
+        p5 = vecs[rng.choice(len(vecs), 5, replace=False)] * 2.0 ** sc
+        p5[4] = with_zero[rng.integers(0, len(with_zero))] * 2.0 ** sc
+        z = int(np.flatnonzero(p5[4] == 0)[0])
+        p5[4, z] = (1.0 if g % 2 else -1.0) * 2.0 ** (sc - 300)   # off the sphere by 2^(2s-600)
+        groups.append(p5)
+    near = np.concatenate(groups)
+    qn = (np.arange(200)[:, None] * 5 + np.arange(5)[None, :]).astype(np.int32)
+    for kind, fn in (("in_sphere", d3.in_sphere), ("in_sphere_unperturbed", d3.in_sphere_unperturbed)):
+        got = fn(near, qn)
+        assert (got != 0).all()
+        assert (got == oracle.exact_predicate(kind, near, qn)).all(), kind
+        assert (got == oracle.ref_predicate(kind, near, qn)).all(), kind
     # Points on a plane through the origin tilted by 2^-800: orient3d exactly
     # resolvable only with about 2400 bits.
     plane = np.array([[1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0], [2.0 ** -800, 0.5, 0.5]])
