@@ -94,6 +94,9 @@ def parse_args():
                          "spatial-sort microbenchmarks, one line each; readers: the host "
                          "input readers on files of a sample of the batched sets (no GPU)")
     ap.add_argument("--n", type=int, default=PLAIN_N, help="points of the plain workload")
+    ap.add_argument("--queries", type=int, default=0,
+                    help="predicates workload: queries of each kind (default 1e8); a smaller count "
+                         "serves one-kernel profiler captures")
     ap.add_argument("--dist", default="uniform", choices=["uniform", "clusters", "lattice", "sphere"],
                     help="distribution of the plain workload")
     ap.add_argument("--schedule", type=int, default=0,
@@ -838,14 +841,15 @@ def run_predicates(args):
     lib = d3.library()
     res = {}
     parity_ok = True
+    nq = args.queries or PRED_QUERIES
     for kind, name, k, base, groups, ops in ((d3.ORIENT3D, "orient3d", 4, pbase, g4, ORIENT3D_OPS),
                                              (d3.IN_SPHERE, "in_sphere", 5, sbase, g5, IN_SPHERE_OPS)):
-        idx = predicate_queries(torch, dev, k, n_uni, base, groups, PRED_QUERIES, 7 + k)
-        out = torch.empty(PRED_QUERIES, dtype=torch.int8, device=dev)
+        idx = predicate_queries(torch, dev, k, n_uni, base, groups, nq, 7 + k)
+        out = torch.empty(nq, dtype=torch.int8, device=dev)
         st = d3._PredStats()
 
         def call():
-            d3._check(lib.d3g_predicates_device(pts.data_ptr(), pts.shape[0], idx.data_ptr(), PRED_QUERIES,
+            d3._check(lib.d3g_predicates_device(pts.data_ptr(), pts.shape[0], idx.data_ptr(), nq,
                                                 kind, out.data_ptr(), ctypes.c_void_p(stream.cuda_stream),
                                                 ctypes.byref(st)), name)
 
@@ -859,10 +863,10 @@ def run_predicates(args):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
-        qps = PRED_QUERIES / (ms / 1000.0)
+        qps = nq / (ms / 1000.0)
         signs = torch.bincount((out.to(torch.int16) + 1).cpu(), minlength=3).tolist()
-        res[name] = {"queries": PRED_QUERIES, "ms": ms, "queries_per_s": qps,
-                     "exact_fraction": st.n_exact / PRED_QUERIES,
+        res[name] = {"queries": nq, "ms": ms, "queries_per_s": qps,
+                     "exact_fraction": st.n_exact / nq,
                      "fp64_ops_per_query": ops, "fp64_ops_per_s": qps * ops,
                      "fp64_frac_of_measured_addmul_peak": qps * ops / addmul,
                      "signs_neg_zero_pos": signs}
@@ -889,7 +893,7 @@ def run_predicates(args):
             parity_ok = parity_ok and res[name]["parity"]["equal"]
         del idx, out
     line = {"metric": "predicate queries/s (filter + exact stage + perturbation)",
-            "value": 2 * PRED_QUERIES / sum(r["ms"] / 1000.0 for r in res.values()),
+            "value": 2 * nq / sum(r["ms"] / 1000.0 for r in res.values()),
             "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"1e8 orient3d + 1e8 in_sphere over a table of 1e7 points uniform in "

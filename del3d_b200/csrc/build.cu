@@ -793,11 +793,19 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
             tv = ld4(T.tv + t);
         }
     }
+    int4 tn = ld4(T.tn + t);
     int prev = -1;
     uint32_t h = uint32_t(pid) * 2654435761u + 12345u;
     const int limit = min(kAsyncWalkLimit, T.walk_limit);
     for (int step = 0; step < limit; ++step) {
-        const int4 tn = ld4(T.tn + t);
+        // While lanes 0-3 test the four facets, lanes 4-7 fetch the four
+        // neighbours' vertices and lanes 8-11 their neighbours: the step to
+        // the chosen neighbour then waits for no further memory read.
+        int4 pre = make_int4(0, 0, 0, 0);
+        if (lane >= 4 && lane < 12) {
+            const int nbr = at(tn, lane & 3) >> 2;
+            pre = lane < 8 ? ld4(T.tv + nbr) : ld4(T.tn + nbr);
+        }
         h = h * 1664525u + 1013904223u;
         const int s0 = int(h >> 30);
         bool neg = false, undecided = false;
@@ -823,11 +831,15 @@ __device__ int walk_async(int t, const Pt& p, int pid, const Tables& T, const do
         const unsigned rot = ((m >> s0) | (m << (4 - s0))) & 0xFu;
         const int i = (s0 + __ffs(int(rot)) - 1) & 3;
         const int next = at(tn, i) >> 2;
-        const int4 nv = ld4(T.tv + next);
+        const int4 nv = make_int4(__shfl_sync(kFull, pre.x, 4 + i), __shfl_sync(kFull, pre.y, 4 + i),
+                                  __shfl_sync(kFull, pre.z, 4 + i), __shfl_sync(kFull, pre.w, 4 + i));
+        const int4 nn = make_int4(__shfl_sync(kFull, pre.x, 8 + i), __shfl_sync(kFull, pre.y, 8 + i),
+                                  __shfl_sync(kFull, pre.z, 8 + i), __shfl_sync(kFull, pre.w, 8 + i));
         if (inf_pos(nv) >= 0) return next;
         prev = t;
         t = next;
         tv = nv;
+        tn = nn;
     }
     return -1;
 }
