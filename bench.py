@@ -115,6 +115,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--parity-every", type=int, default=0,
+                    help="parity leg: check the cells of every k-th set (default 64; 1 checks every set)")
     ap.add_argument("--profile-run", action="store_true",
                     help="warm-up and timed steps only (no other legs): the command profiled by ncu")
     return ap.parse_args()
@@ -305,7 +307,7 @@ def cpu_baseline_leg(sets):
 PARITY_EVERY = 64
 
 
-def parity_leg(sets, gpu_cells):
+def parity_leg(sets, gpu_cells, every=PARITY_EVERY):
     """Parity: the cells the timed batched build gave every PARITY_EVERY-th
     set (`gpu_cells`: set index -> host array) against the reference's build of
     that set (oracle/_ref), put in the same canonical order; one set per host
@@ -327,7 +329,7 @@ def parity_leg(sets, gpu_cells):
     return {"sets": len(idx), "points": int(sum(sets[k].shape[0] for k in idx)), "equal": all(ok),
             "mismatched_sets": [k for k, o in zip(idx, ok) if not o][:10],
             "method": "the reference build (oracle/_ref) of every "
-                       f"{PARITY_EVERY}th set, canonical order, against the timed build's cells"}
+                       f"{every}th set, canonical order, against the timed build's cells"}
 
 
 def run_reference(args):
@@ -559,7 +561,8 @@ def run_ours(args):
     # After the timed region: the cells of a sample of sets, for the parity check.
     par_cells = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_run:
-        par_cells = {k: cells[int(co[k]):int(co[k + 1])].cpu().numpy() for k in range(0, len(sets), PARITY_EVERY)}
+        every = args.parity_every or PARITY_EVERY
+        par_cells = {k: cells[int(co[k]):int(co[k + 1])].cpu().numpy() for k in range(0, len(sets), every)}
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1) / args.steps
@@ -706,7 +709,7 @@ def run_ours(args):
             line["serving"] = serving_leg(torch, d3)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_leg(sets)
-            line["parity"] = parity_leg(sets, par_cells)
+            line["parity"] = parity_leg(sets, par_cells, args.parity_every or PARITY_EVERY)
     if rank == 0:
         # The figures of the headline metric, last in the line.
         srv = (line.get("serving") or {}).get("sweep") or []

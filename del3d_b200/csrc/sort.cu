@@ -221,6 +221,40 @@ __global__ void k_final_sets(const int32_t* __restrict__ j, const int32_t* __res
     }
 }
 
+/// Sets of at most this many points are shuffled by the reference's loop itself,
+/// one thread per set over the set's sequence in shared memory: for a few
+/// thousand points that is far quicker than the parallel machinery above,
+/// whose fixed cost is several kernels and host round trips.
+constexpr int kSerialShuffleMax = 8192;
+
+/// rand48.h:146-153 with the engine seeded to 1, verbatim: element k (1..n-1)
+/// swapped with element j drawn uniformly from [0, k] by the bucket reduction of
+/// rand48.h:115-127 (draw r, j = r / (2^31 / (k+1)), redrawn while j > k).
+__global__ void k_shuffle_serial(const int64_t* __restrict__ off, int32_t* __restrict__ order) {
+    __shared__ int32_t a[kSerialShuffleMax];
+    const int s = blockIdx.x;
+    const int64_t base = off[s];
+    const int n = int(off[s + 1] - base);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t x = kSeedState;
+        for (int k = 1; k < n; ++k) {
+            const uint32_t bucket = uint32_t((uint64_t(1) << 31) / uint64_t(k + 1));
+            uint32_t j;
+            do {
+                x = (kA * x + kC) & kMask;
+                j = uint32_t(x >> 17) / bucket;
+            } while (j > uint32_t(k));
+            const int32_t t = a[k];
+            a[k] = a[j];
+            a[j] = t;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) order[base + i] = a[i];
+}
+
 // ---- the Hilbert median splits (spatial_sort.cpp:40-117) -------------------------
 //
 // Every split position is begin + (end - begin) / 2 whatever the data, so the
@@ -638,6 +672,11 @@ int shuffle_sets_device(const int64_t* h_off, const int64_t* d_off, int nsets, i
     for (int i = 0; i < nsets; ++i) n = std::max<int64_t>(n, h_off[i + 1] - h_off[i]);
     const int64_t total = h_off[nsets] - h_off[0];
     if (total <= 0) return D3G_OK;
+    if (n <= kSerialShuffleMax) {
+        k_shuffle_serial<<<unsigned(nsets), 128, 0, s>>>(d_off, d_order);
+        D3G_CUDA(cudaGetLastError());
+        return D3G_OK;
+    }
     JumpTable jt;
     jt.step[0] = Affine{kA, kC};
     for (int i = 1; i < 48; ++i) jt.step[i] = compose(jt.step[i - 1], jt.step[i - 1]);
