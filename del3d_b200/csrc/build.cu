@@ -94,6 +94,7 @@ struct Tables {
     int* tet_count;
     int cap;
     int walk_limit;            // steps of a lockstep walk before ST_WALK_LIMIT
+    const int32_t* vset;       // the point set of each vertex (batched builds share the tables)
 };
 
 struct Workers {
@@ -1042,11 +1043,15 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         if (!try_lock(A.lock, seed, region, &seen)) {
             res = 1;
         } else {
+            // The walk read tets other warps were rewriting: a tet read half
+            // written (vertices new, neighbours not yet) can send it on through a
+            // slot not yet filled in - into another set's tets in a batched
+            // build.  Only a live tet of v's own set can seed the region.
             int r = 0;
-            if (__ldcg(T.alive + seed)) {
-                if (kFast) r = in_conflict_fast(ld4(T.tv + seed), p, v, vx, ex);
-                if (!kFast || (r & CT_UNDECIDED))
-                    r = conflict_test_seed(ld4(T.tv + seed), p.x, p.y, p.z, v, vx, ex, st);
+            const int4 stv = ld4(T.tv + seed);
+            if (__ldcg(T.alive + seed) && T.vset[stv.x != kInf ? stv.x : stv.y] == T.vset[v]) {
+                if (kFast) r = in_conflict_fast(stv, p, v, vx, ex);
+                if (!kFast || (r & CT_UNDECIDED)) r = conflict_test_seed(stv, p.x, p.y, p.z, v, vx, ex, st);
                 ctr.count(r);
             }
             if (r & CT_IN) {
@@ -1125,9 +1130,11 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
                     const int f = fac[k];
                     unlock_if(A.lock, at(ld4(T.tn + (f >> 2)), f & 3) >> 2, ring);
                 }
-                for (int k = lane; k < npend; k += 32) {
-                    const int f = fac[W.fac_cap - 1 - k];
-                    unlock_if(A.lock, at(ld4(T.tn + (f >> 2)), f & 3) >> 2, pending);
+                if (kFast) {
+                    for (int k = lane; k < npend; k += 32) {
+                        const int f = fac[W.fac_cap - 1 - k];
+                        unlock_if(A.lock, at(ld4(T.tn + (f >> 2)), f & 3) >> 2, pending);
+                    }
                 }
                 __syncwarp();
                 for (int k = lane; k < ncav; k += 32) unlock_if(A.lock, cav[k], region);
@@ -1414,6 +1421,7 @@ enum : int {
     VF_FACET = 4,       // two neighbours whose shared facets have different vertices
     VF_LOCK = 5,        // a tet still locked after the asynchronous passes
     VF_VERT_TET = 6,    // an inserted vertex whose tet is dead or does not contain it
+    VF_SET = 7,         // a tet whose vertices belong to different point sets
 };
 
 /// One thread per tet slot, then one per vertex: checks what the reference's
@@ -1442,6 +1450,11 @@ __global__ void k_validate(Tables T, const int* __restrict__ lock, int ntet, int
                 detail = k;
             }
             if (!code && ninf > 1) code = VF_VERTEX;
+            if (!code) {
+                const int s0 = T.vset[tv.x != kInf ? tv.x : tv.y];
+                for (int k = 0; k < 4; ++k)
+                    if (at(tv, k) != kInf && T.vset[at(tv, k)] != s0) code = VF_SET;
+            }
             for (int k = 0; k < 4 && !code; ++k) {
                 detail = k;
                 const int e = at(tn, k);
@@ -2252,6 +2265,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     T.fnew = fnew.p;
     T.vert_tet = vert_tet.p;
     T.tet_count = tet_count.p;
+    T.vset = vset.p;
     k_set_int<<<1, 1, 0, s>>>(tet_count.p, 5 * nsets);
     k_init_tets<<<grid_for(nsets, 64), 64, 0, s>>>(T, vx.p, skips.p, nsets, status.p);
     // Sets whose coordinates span few bits (integer lattices, coarse grids):
@@ -2463,11 +2477,12 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         D3G_CUDA(cudaStreamSynchronize(s));
         if (rec == ~0ull) return D3G_OK;
         static const char* what[] = {"", "bad vertex", "bad neighbour", "neighbour does not point back",
-                                     "neighbours' shared facets differ", "lock held", "vertex's tet"};
+                                     "neighbours' shared facets differ", "lock held", "vertex's tet",
+                                     "vertices of different sets"};
         const int code = int(rec >> 60);
         char msg[200];
         std::snprintf(msg, sizeof msg, "d3g_build: validate %s level %d: %s (%s %lld, %lld)", when, lev,
-                      what[code > 0 && code < 7 ? code : 0], code == VF_VERT_TET ? "vertex" : "tet",
+                      what[code > 0 && code < 8 ? code : 0], code == VF_VERT_TET ? "vertex" : "tet",
                       (long long)((rec >> 30) & 0x3FFFFFFFull), (long long)(rec & 0x3FFFFFFFull));
         set_error(msg);
         return D3G_ERR_INTERNAL;
@@ -2934,7 +2949,10 @@ void d3g_options_default(d3g_options* o) {
     o->tet_capacity = 0;
     o->walk_limit = 0;
     o->cavity_capacity = 0;
-    o->validate = 0;
+    // D3G_VALIDATE=1 in the environment turns the device self-check on for every
+    // build that takes the defaults (as the reference's DEL3D_VALIDATE builds do).
+    const char* val = getenv("D3G_VALIDATE");
+    o->validate = (val && val[0] && val[0] != '0') ? 1 : 0;
     d3g_tuning t;
     if (current_tuning(&t)) {
         o->schedule = t.schedule;
