@@ -559,8 +559,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop() if clocks else None
     # After the timed region: the cells of a sample of sets, for the parity check.
+    # Every rank checks the sets it built (their parity is combined below).
     par_cells = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile_run:
+    if not args.no_cpu_baseline and not args.profile_run:
         every = args.parity_every or PARITY_EVERY
         par_cells = {k: cells[int(co[k]):int(co[k + 1])].cpu().numpy() for k in range(0, len(sets), every)}
     if dist:
@@ -702,6 +703,22 @@ def run_ours(args):
         }
     if dist:
         dist.barrier()
+    # Parity on every rank, over its own sets; with several ranks the outcome is
+    # combined (every rank takes part in the same reduction) and any mismatch
+    # fails the run on every rank.
+    parity = None
+    if par_cells is not None:
+        parity = parity_leg(sets, par_cells, args.parity_every or PARITY_EVERY)
+        if dist:
+            flags = torch.tensor([0.0 if parity is None else float(not parity["equal"]),
+                                  0.0 if parity is None else float(parity["sets"]),
+                                  0.0 if parity is None else float(parity["points"])],
+                                 dtype=torch.float64, device=dev)
+            dist.all_reduce(flags, op=dist.ReduceOp.SUM)
+            if parity is not None:
+                parity = dict(parity, ranks=world, sets=int(flags[1].item()), points=int(flags[2].item()),
+                              equal=flags[0].item() == 0.0,
+                              mismatched_sets=parity["mismatched_sets"] if rank == 0 else [])
     if rank == 0 and world == 1:
         if not args.no_plain:
             line["plain_1e7"] = plain_1e7_leg(torch, d3, dev, stream, not args.no_cpu_baseline)
@@ -709,7 +726,8 @@ def run_ours(args):
             line["serving"] = serving_leg(torch, d3)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_leg(sets)
-            line["parity"] = parity_leg(sets, par_cells, args.parity_every or PARITY_EVERY)
+    if rank == 0 and parity is not None:
+        line["parity"] = parity
     if rank == 0:
         # The figures of the headline metric, last in the line.
         srv = (line.get("serving") or {}).get("sweep") or []
@@ -731,8 +749,9 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    if rank == 0 and line.get("parity") and not line["parity"]["equal"]:
-        print("bench: the timed build's cells differ from the reference's", file=sys.stderr)
+    if parity is not None and not parity["equal"]:
+        if rank == 0:
+            print("bench: the timed build's cells differ from the reference's", file=sys.stderr)
         return 1
     return 0
 

@@ -729,6 +729,13 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
 // tet data that other warps write goes to L2 (__ldcg), not the SM's L1.
 
 constexpr int kAsyncRetries = 6;
+// Chunks of sets whose filters are exact go whole to the full variant (1), or
+// through the fast one, whose undecided hull in-circle tests are then resolved
+// after its growth loop (0).
+#ifndef D3G_PASS_EXACT_CHUNKS
+#define D3G_PASS_EXACT_CHUNKS 1
+#endif
+constexpr bool kPassExactChunks = D3G_PASS_EXACT_CHUNKS != 0;
 constexpr int kAsyncWalkLimit = 1 << 14;
 
 struct AsyncCtx {
@@ -1356,7 +1363,7 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
         const int wq = int((int64_t(q) * A.stride) % A.nw);
         const int w = A.wlist ? A.wlist[wq] : wq;
         const bool ex = W.set_exact[W.wset[w]] != 0;
-        if (kFast && ex) {
+        if (kFast && ex && kPassExactChunks) {
             // A set whose coordinates make the filters exact (integer lattices,
             // coarse grids) needs the hull in-circle test wherever points lie in
             // the planes of hull facets - much of the time: its chunks go whole
