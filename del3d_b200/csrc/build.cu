@@ -730,8 +730,8 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
 
 constexpr int kAsyncRetries = 6;
 // Chunks of sets whose filters are exact go whole to the full variant (1), or
-// through the fast one, whose undecided hull in-circle tests are then resolved
-// after its growth loop (0).
+// through the fast one, which defers every point whose tests its filters leave
+// undecided to the full variant's pass (0).
 #ifndef D3G_PASS_EXACT_CHUNKS
 #define D3G_PASS_EXACT_CHUNKS 1
 #endif
@@ -1026,11 +1026,8 @@ template <bool kFast>
 __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, const AsyncCtx& A,
                             const double* __restrict__ vx, bool ex, uint32_t* st, int slot, int lane,
                             unsigned long long* nC, unsigned long long* nF, const SharedCounters& ctr) {
-    // Lock values of this warp: region tets, tets across the region boundary
-    // (ring), and - fast variant - tets whose conflict test the filters left
-    // undecided (pending, decided after the growth loop by the full test).
     const int owner = slot + 1;
-    const int region = owner << 2, ring = region | 1, pending = region | 2;
+    const int region = owner << 1, ring = region | 1;
     const Pt p = vpt(vx, v);
     const int seed = walk_async<kFast>(t0, p, v, T, vx, ex, st, lane);
     if (kFast && seed == -2) {
@@ -1058,149 +1055,84 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             const int4 stv = ld4(T.tv + seed);
             if (__ldcg(T.alive + seed) && T.vset[stv.x != kInf ? stv.x : stv.y] == T.vset[v]) {
                 if (kFast) r = in_conflict_fast(stv, p, v, vx, ex);
-                if (!kFast || (r & CT_UNDECIDED)) r = conflict_test_seed(stv, p.x, p.y, p.z, v, vx, ex, st);
+                else r = conflict_test_seed(stv, p.x, p.y, p.z, v, vx, ex, st);
                 ctr.count(r);
             }
             if (r & CT_IN) {
                 cav[0] = seed;
             } else {
                 unlock_if(A.lock, seed, region);
-                res = 2;
+                res = (r & CT_UNDECIDED) ? 3 : 2;
             }
         }
     }
     res = __shfl_sync(kFull, res, 0);
     if (res != 0) {
-        if (lane == 0) atomicAdd(A.stats + (res == 1 ? 0 : 2), 1ull);
-        return AI_RETRY;
+        if (lane == 0) atomicAdd(A.stats + (res == 1 ? 0 : (res == 2 ? 2 : 6)), 1ull);
+        return res == 3 ? AI_DEFER : AI_RETRY;
     }
     __syncwarp();
     const unsigned lt = (1u << lane) - 1u;
-    // Region tets cav[0, ncav) (grown breadth-first from cav[head]), boundary
-    // facets fac[0, nfac) (region tet * 4 + facet), and - fast variant - the
-    // facets whose outside tet is pending, stored from the end of fac:
-    // fac[fac_cap - 1 - k] for k < npend.
-    int ncav = 1, nfac = 0, head = 0, npend = 0;
+    int ncav = 1, nfac = 0, head = 0;
     int outcome = AI_DONE;
-    for (;;) {
-        while (head < ncav) {
-            const int nproc = min(ncav - head, 8);
-            const bool valid = (lane >> 2) < nproc;
-            const int i = lane & 3;
-            int c = 0, nb = 0, kind = 0, got = -1;   // got: a tet this lane locked in this step
-            bool abort = false;
-            if (valid) {
-                c = cav[head + (lane >> 2)];
-                nb = at(ld4(T.tn + c), i) >> 2;
-                int seen = 0;
-                if (try_lock(A.lock, nb, ring, &seen)) {
-                    got = nb;
-                    int r;
-                    if (kFast) r = in_conflict_fast(ld4(T.tv + nb), p, v, vx, ex);
-                    else r = conflict_test(ld4(T.tv + nb), p, v, vx, ex, st);
-                    if (r & CT_IN) {
-                        LockRef(A.lock[nb]).store(region, cuda::memory_order_relaxed);
-                        kind = 2;
-                    } else if (kFast && (r & CT_UNDECIDED)) {
-                        LockRef(A.lock[nb]).store(pending, cuda::memory_order_relaxed);
-                        kind = 4;
-                    } else {
-                        kind = 1;
-                    }
-                    if (!(r & CT_UNDECIDED)) ctr.count(r);
-                } else if (seen == region) {
-                    kind = 0;                             // already in the region
-                } else if (seen == ring || seen == pending) {
-                    kind = 3;                             // locked by us: decided below
+    while (head < ncav) {
+        const int nproc = min(ncav - head, 8);
+        const bool valid = (lane >> 2) < nproc;
+        const int i = lane & 3;
+        int c = 0, nb = 0, kind = 0, got = -1;   // got: a tet this lane locked in this step
+        bool abort = false, undecided = false;
+        if (valid) {
+            c = cav[head + (lane >> 2)];
+            nb = at(ld4(T.tn + c), i) >> 2;
+            int seen = 0;
+            if (try_lock(A.lock, nb, ring, &seen)) {
+                got = nb;
+                int r;
+                if (kFast) r = in_conflict_fast(ld4(T.tv + nb), p, v, vx, ex);
+                else r = conflict_test(ld4(T.tv + nb), p, v, vx, ex, st);
+                ctr.count(r);
+                if (r & CT_IN) {
+                    LockRef(A.lock[nb]).store(region, cuda::memory_order_relaxed);
+                    kind = 2;
                 } else {
-                    abort = true;                         // another warp holds it
+                    kind = 1;                             // undecided: held as ring
+                    undecided = (r & CT_UNDECIDED) != 0;
                 }
+            } else if (seen == region) {
+                kind = 0;                                 // already in the region
+            } else if (seen == ring) {
+                kind = 3;                                 // locked by us this step: decided below
+            } else {
+                abort = true;                             // another warp holds it
             }
-            __syncwarp();
-            if (kind == 3) {
-                // Another lane may have just turned it into a region or pending tet.
-                const int now = __ldcg(A.lock + nb);
-                kind = now == region ? 0 : (now == pending ? 4 : 1);
-            }
-            const bool ab = __any_sync(kFull, abort);
-            const unsigned mc = __ballot_sync(kFull, kind == 2);
-            const unsigned mf = __ballot_sync(kFull, kind == 1);
-            const unsigned mp = kFast ? __ballot_sync(kFull, kind == 4) : 0u;
-            const bool full = ncav + __popc(mc) > W.cav_cap ||
-                              nfac + __popc(mf) + npend + __popc(mp) > W.fac_cap;
-            if (ab || full) {
-                // Give everything back: this step's new locks, the region, the
-                // ring, the pending tets.
-                if (got >= 0) unlock_if(A.lock, got, kind == 2 ? region : (kind == 4 ? pending : ring));
-                __syncwarp();
-                for (int k = lane; k < nfac; k += 32) {
-                    const int f = fac[k];
-                    unlock_if(A.lock, at(ld4(T.tn + (f >> 2)), f & 3) >> 2, ring);
-                }
-                if (kFast) {
-                    for (int k = lane; k < npend; k += 32) {
-                        const int f = fac[W.fac_cap - 1 - k];
-                        unlock_if(A.lock, at(ld4(T.tn + (f >> 2)), f & 3) >> 2, pending);
-                    }
-                }
-                __syncwarp();
-                for (int k = lane; k < ncav; k += 32) unlock_if(A.lock, cav[k], region);
-                if (lane == 0) atomicAdd(A.stats + (ab ? 0 : 3), 1ull);
-                outcome = ab ? AI_RETRY : AI_LEAVE;
-                break;
-            }
-            if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
-            if (kind == 1) fac[nfac + __popc(mf & lt)] = c * 4 + i;
-            if (kFast && kind == 4) fac[W.fac_cap - 1 - (npend + __popc(mp & lt))] = c * 4 + i;
-            ncav += __popc(mc);
-            nfac += __popc(mf);
-            npend += __popc(mp);
-            head += nproc;
-            __syncwarp();
         }
-        if (!kFast || outcome != AI_DONE || npend == 0) break;
-        // The pending facets, one at a time: the first time a pending tet comes
-        // up, the full conflict test (out of line, outside the growth loop, so
-        // that the loop keeps its state in registers) makes it a region or a
-        // ring tet; every pending facet then becomes an internal facet or a
-        // boundary facet.  New region tets send the growth round again.
-        for (int k = 0; k < npend; ++k) {
-            const int f = fac[W.fac_cap - 1 - k];
-            const int nb = at(ld4(T.tn + (f >> 2)), f & 3) >> 2;
-            int now = __ldcg(A.lock + nb);
-            if (now == pending) {
-                int r = 0;
-                if (lane == 0) {
-                    r = conflict_test_seed(ld4(T.tv + nb), p.x, p.y, p.z, v, vx, ex, st);
-                    ctr.count(r);
-                }
-                r = __shfl_sync(kFull, r, 0);
-                now = (r & CT_IN) ? region : ring;
-                if (lane == 0) {
-                    LockRef(A.lock[nb]).store(now, cuda::memory_order_relaxed);
-                    if (now == region) cav[ncav] = nb;
-                }
-                if (now == region) ++ncav;
-            }
-            if (now == ring) {
-                if (lane == 0) fac[nfac] = f;
-                ++nfac;
-            }
-            __syncwarp();
-        }
-        npend = 0;
-        if (ncav > W.cav_cap) {   // the region outgrew the scratch (fac cannot: it held the pending)
+        __syncwarp();
+        if (kind == 3) kind = __ldcg(A.lock + nb) == region ? 0 : 1;
+        const bool ab = __any_sync(kFull, abort);
+        const bool und = kFast && __any_sync(kFull, undecided);
+        const unsigned mc = __ballot_sync(kFull, kind == 2);
+        const unsigned mf = __ballot_sync(kFull, kind == 1);
+        const bool full = ncav + __popc(mc) > W.cav_cap || nfac + __popc(mf) > W.fac_cap;
+        if (ab || full || und) {
+            // Give everything back: this step's new locks, the region, the ring.
+            if (got >= 0) unlock_if(A.lock, got, kind == 2 ? region : ring);
             __syncwarp();
             for (int k = lane; k < nfac; k += 32) {
                 const int f = fac[k];
                 unlock_if(A.lock, at(ld4(T.tn + (f >> 2)), f & 3) >> 2, ring);
             }
             __syncwarp();
-            for (int k = lane; k < min(ncav, W.cav_cap); k += 32) unlock_if(A.lock, cav[k], region);
-            if (lane == 0) atomicAdd(A.stats + 3, 1ull);
-            outcome = AI_LEAVE;
+            for (int k = lane; k < ncav; k += 32) unlock_if(A.lock, cav[k], region);
+            if (lane == 0) atomicAdd(A.stats + (ab ? 0 : (und ? 6 : 3)), 1ull);
+            outcome = ab ? AI_RETRY : (und ? AI_DEFER : AI_LEAVE);
             break;
         }
+        if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
+        if (kind == 1) fac[nfac + __popc(mf & lt)] = c * 4 + i;
+        ncav += __popc(mc);
+        nfac += __popc(mf);
+        head += nproc;
+        __syncwarp();
     }
     if (outcome != AI_DONE) return outcome;
 
