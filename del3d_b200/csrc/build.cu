@@ -2664,6 +2664,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 D3G_CUDA(cudaStreamSynchronize(s));
                 R.stats.launches_async += 1;
                 R.stats.async_inserted += int64_t(won1 - won0);
+                if (trace)
+                    fprintf(stderr, "d3g level %d async pass %s chunks-or-points %d inserted %llu left %d\n", lev,
+                            fast ? "fast" : "full", nw, won1 - won0, *nleft_out);
                 if (opt.timing) {
                     float am = 0.f;
                     cudaEventElapsedTime(&am, kev[0], kev[1]);
