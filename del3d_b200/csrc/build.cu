@@ -733,7 +733,7 @@ constexpr int kAsyncRetries = 6;
 // through the fast one, which defers every point whose tests its filters leave
 // undecided to the full variant's pass (0).
 #ifndef D3G_PASS_EXACT_CHUNKS
-#define D3G_PASS_EXACT_CHUNKS 1
+#define D3G_PASS_EXACT_CHUNKS 0
 #endif
 constexpr bool kPassExactChunks = D3G_PASS_EXACT_CHUNKS != 0;
 constexpr int kAsyncWalkLimit = 1 << 14;
@@ -963,14 +963,92 @@ __device__ __forceinline__ InSphereFilter in_sphere_filter_lean(const Pt& a, con
     return r;
 }
 
+/// coplanar_orientation3 (the first non-zero orient2d of the xy, yz and xz
+/// projections) for a set whose coordinates make the orient2d determinants
+/// exact in double: each is the sign of its determinant.
+__device__ __forceinline__ int coplanar_orientation3_ex(const Pt& p, const Pt& q, const Pt& r) {
+    int o = sign_of(fsub(fmul(fsub(q.x, p.x), fsub(r.y, p.y)), fmul(fsub(q.y, p.y), fsub(r.x, p.x))));
+    if (o != 0) return o;
+    o = sign_of(fsub(fmul(fsub(q.y, p.y), fsub(r.z, p.z)), fmul(fsub(q.z, p.z), fsub(r.y, p.y))));
+    if (o != 0) return o;
+    return sign_of(fsub(fmul(fsub(q.x, p.x), fsub(r.z, p.z)), fmul(fsub(q.z, p.z), fsub(r.x, p.x))));
+}
+
+/// The cocircular tie-break (reference src/predicates2.cpp:241-258) of four
+/// distinct vertices va, vb, vd, pid of such a set: walking down their
+/// lexicographic order from the largest, the first that is pid gives NEGATIVE;
+/// the first other one whose replacement by pid gives a non-zero coplanar
+/// orientation gives it times the orientation of (va, vb, vd); else the
+/// opposite of that orientation.  Points are read again from memory, as in
+/// in_sphere_tiebreak_ex.
+__device__ __forceinline__ int in_circle_tiebreak_ex(int va, int vb, int vd, int pid,
+                                                     const double* __restrict__ vx) {
+    const int local = coplanar_orientation3_ex(ld_vertex(vx, va), ld_vertex(vx, vb), ld_vertex(vx, vd));
+    unsigned excluded = 0;
+#pragma unroll 1
+    for (int r = 0; r < 3; ++r) {
+        int best = -1;
+        Pt bp{0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int k = 0; k < 4; ++k) {
+            if (excluded & (1u << k)) continue;
+            const Pt q = ld_vertex(vx, k == 0 ? va : (k == 1 ? vb : (k == 2 ? vd : pid)));
+            if (best < 0 || !lexico_less(q, bp)) {   // a later slot wins ties
+                best = k;
+                bp = q;
+            }
+        }
+        excluded |= 1u << best;
+        if (best == 3) return -1;
+        const Pt pp = ld_vertex(vx, pid);
+        const Pt A = best == 0 ? pp : ld_vertex(vx, va), B = best == 1 ? pp : ld_vertex(vx, vb),
+                 C = best == 2 ? pp : ld_vertex(vx, vd);
+        const int o = coplanar_orientation3_ex(A, B, C);
+        if (o != 0) return o * local;
+    }
+    return -local;
+}
+
+/// The hull in-circle test (reference src/triangulation.cpp:588-602, a point
+/// in the plane of the hull facet (va, vb, vd) of infinite tet `tet`: in
+/// conflict iff inside the facet's circumcircle, a tie by the cocircular
+/// perturbation) for a set whose coordinates make the filters exact, without
+/// the in-circle determinant: the sphere through va, vb, vd and the apex x of
+/// the finite tet across the facet cuts the facet's plane in the facet's
+/// circumcircle, and a point of that plane has the same power with respect
+/// to both, so sign in_circle(va, vb, vd, p) = sign det_in_sphere(va, vb, vd,
+/// x, p) * sign det_orient3d(va, vb, vd, x), both exact here.  The caller
+/// holds the lock of `tet`, so the finite tet across its facet is not being
+/// rewritten.  Returns 1 (inside), -1 (outside), or 0 if the apex is unusable
+/// (the caller then leaves the test undecided).
+__device__ __forceinline__ int hull_in_circle_ex(const Tables& T, int tet, int ip, int va, int vb, int vd, int pid,
+                                                 const double* __restrict__ vx) {
+    const int f = at(ld4(T.tn + tet), ip) >> 2;
+    const int4 fv = ld4(T.tv + f);
+    int x = -1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int w = at(fv, k);
+        if (w != va && w != vb && w != vd) x = w;
+    }
+    if (x < 0) return 0;   // kInf is negative
+    const Pt a = ld_vertex(vx, va), b = ld_vertex(vx, vb), d = ld_vertex(vx, vd), xp = ld_vertex(vx, x);
+    const int so = sign_of(orient3d_filter(a, b, d, xp).det);
+    if (so == 0) return 0;
+    const int ss = sign_of(in_sphere_filter_lean(a, b, d, xp, ld_vertex(vx, pid)).det);
+    if (ss != 0) return ss * so;
+    return in_circle_tiebreak_ex(va, vb, vd, pid, vx);
+}
+
 /// The conflict test of the fast variant (reference src/triangulation.cpp:588-602,
-/// as conflict_test), with its outcome bits; CT_UNDECIDED when the filter cannot
-/// decide and the exact stage is needed, or the point lies in the plane of a
-/// hull facet (the coplanar in-circle test).  Call-free: an exactly cospherical
-/// call on a set whose coordinates make the filter exact gets its tie-break
-/// inline.
-__device__ __forceinline__ int in_conflict_fast(const int4 t, const Pt& p, int pid, const double* __restrict__ vx,
-                                                bool ex) {
+/// as conflict_test) of tet `tet` = t, with its outcome bits; CT_UNDECIDED when
+/// the filter cannot decide and the exact stage is needed, or the point lies in
+/// the plane of a hull facet (the coplanar in-circle test) of a set whose
+/// filters are not exact.  Call-free: on a set whose coordinates make the
+/// filters exact, an exactly cospherical call gets its tie-break inline, and
+/// a point in the plane of a hull facet its in-circle test.
+__device__ __forceinline__ int in_conflict_fast(const Tables& T, int tet, const int4 t, const Pt& p, int pid,
+                                                const double* __restrict__ vx, bool ex) {
     const int ip = inf_pos(t);
     if (ip >= 0) {
         const int o0 = ip == 0 ? 2 : (ip == 1 ? 2 : (ip == 2 ? 1 : 0));
@@ -980,6 +1058,10 @@ __device__ __forceinline__ int in_conflict_fast(const int4 t, const Pt& p, int p
         const Orient3dFilter f = orient3d_filter(a, b, d, p);
         if (f.certain) return f.det < 0.0 ? CT_IN : 0;   // orient3d = -sign(det)
         if (ex && f.det != 0.0) return (f.det < 0.0 ? CT_IN : 0) | CT_UNCERTAIN;
+        if (ex) {
+            const int h = hull_in_circle_ex(T, tet, ip, at(t, o0), at(t, o1), at(t, o2), pid, vx);
+            if (h != 0) return (h > 0 ? CT_IN : 0) | CT_UNCERTAIN | CT_TIE;
+        }
         return CT_UNDECIDED;
     }
     const Pt a = vpt(vx, t.x), b = vpt(vx, t.y), c = vpt(vx, t.z), d = vpt(vx, t.w);
@@ -1054,7 +1136,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             int r = 0;
             const int4 stv = ld4(T.tv + seed);
             if (__ldcg(T.alive + seed) && T.vset[stv.x != kInf ? stv.x : stv.y] == T.vset[v]) {
-                if (kFast) r = in_conflict_fast(stv, p, v, vx, ex);
+                if (kFast) r = in_conflict_fast(T, seed, stv, p, v, vx, ex);
                 else r = conflict_test_seed(stv, p.x, p.y, p.z, v, vx, ex, st);
                 ctr.count(r);
             }
@@ -1088,7 +1170,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             if (try_lock(A.lock, nb, ring, &seen)) {
                 got = nb;
                 int r;
-                if (kFast) r = in_conflict_fast(ld4(T.tv + nb), p, v, vx, ex);
+                if (kFast) r = in_conflict_fast(T, nb, ld4(T.tv + nb), p, v, vx, ex);
                 else r = conflict_test(ld4(T.tv + nb), p, v, vx, ex, st);
                 ctr.count(r);
                 if (r & CT_IN) {
