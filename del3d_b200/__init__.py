@@ -104,7 +104,7 @@ class _Options(ctypes.Structure):
     _fields_ = [("want_all_cells", _I32), ("want_incident", _I32), ("chunk", _I32),
                 ("max_rounds", _I32), ("timing", _I32), ("alpha_small", _I32), ("split", _I32),
                 ("lanes", _I32), ("schedule", _I32), ("tet_capacity", _I32), ("walk_limit", _I32),
-                ("cavity_capacity", _I32), ("validate", _I32)]
+                ("cavity_capacity", _I32), ("validate", _I32), ("level_growth", _I32)]
 
 
 class _BatchResult(ctypes.Structure):
@@ -499,7 +499,8 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: Optional[int] = N
                  stats: Optional[dict] = None, alpha_small: Optional[int] = None, split: Optional[int] = None,
                  lanes: Optional[int] = None, schedule: Optional[int] = None, max_rounds: Optional[int] = None,
                  tet_capacity: Optional[int] = None, walk_limit: Optional[int] = None,
-                 cavity_capacity: Optional[int] = None, validate: Optional[bool] = None):
+                 cavity_capacity: Optional[int] = None, validate: Optional[bool] = None,
+                 level_growth: Optional[int] = None):
     """Builds from a device-resident torch tensor (n, 3) float64 on `stream`
     (a raw cudaStream_t handle; 0 = default) and returns the canonical finite
     cells as a device int32 tensor view (n_cells, 4) and the vertex count.
@@ -520,7 +521,8 @@ def build_device(points_dev, out=None, stream: int = 0, chunk: Optional[int] = N
     lib.d3g_options_default(ctypes.byref(opts))
     _apply(opts, chunk=chunk, timing=int(timing), alpha_small=alpha_small, split=split, lanes=lanes,
            schedule=schedule, max_rounds=max_rounds, tet_capacity=tet_capacity, walk_limit=walk_limit,
-           cavity_capacity=cavity_capacity, validate=None if validate is None else int(validate))
+           cavity_capacity=cavity_capacity, validate=None if validate is None else int(validate),
+           level_growth=level_growth)
     st = BuildStats()
     _check(lib.d3g_build_device(x.data_ptr(), n, ctypes.byref(opts), out.data_ptr(), out.shape[0],
                                 ctypes.byref(nc), ctypes.byref(nv), _P(stream), ctypes.byref(st)),
@@ -565,7 +567,8 @@ def build_batch(sets, chunk: int = 0, stats: Optional[dict] = None):
 def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk: Optional[int] = None,
                        stats: Optional[dict] = None, alpha_small: Optional[int] = None,
                        split: Optional[int] = None, lanes: Optional[int] = None,
-                       schedule: Optional[int] = None, validate: Optional[bool] = None):
+                       schedule: Optional[int] = None, validate: Optional[bool] = None,
+                       level_growth: Optional[int] = None):
     """Device-resident form of build_batch: `points_dev` (n, 3) float64 CUDA
     tensor holding the sets back to back, `set_offsets` (n_sets + 1) host
     int64.  Returns the device cells tensor (all sets), the cell offsets per
@@ -584,7 +587,7 @@ def build_batch_device(points_dev, set_offsets, out=None, stream: int = 0, chunk
     opts = _Options()
     lib.d3g_options_default(ctypes.byref(opts))
     _apply(opts, chunk=chunk, alpha_small=alpha_small, split=split, lanes=lanes, schedule=schedule,
-           validate=None if validate is None else int(validate))
+           validate=None if validate is None else int(validate), level_growth=level_growth)
     st = BuildStats()
     _check(lib.d3g_build_batch_device(x.data_ptr(), _ptr(offs), nsets, ctypes.byref(opts), out.data_ptr(),
                                       out.shape[0], _ptr(co), _ptr(nv), _P(stream), ctypes.byref(st)),

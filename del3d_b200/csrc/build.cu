@@ -47,8 +47,8 @@ namespace d3g {
 
 int spatial_order_device(const double* d_xyz, int64_t n, int32_t* d_order, cudaStream_t s);
 int spatial_order_sets_device(const double* d_xyz, const int64_t* h_off, const int64_t* d_off, int nsets,
-                              int32_t* d_order, cudaStream_t s);
-int multiscale_bounds(int64_t n, int64_t* b, int cap);
+                              int32_t* d_order, cudaStream_t s, double level_ratio = 0.125);
+int multiscale_bounds(int64_t n, int64_t* b, int cap, double ratio = 0.125);
 
 namespace {
 
@@ -729,6 +729,8 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
 // tet data that other warps write goes to L2 (__ldcg), not the SM's L1.
 
 constexpr int kAsyncRetries = 6;
+// Passes of the full variant over a level's left points before the rounds.
+constexpr int kLeftPasses = 8;
 // Chunks of sets whose filters are exact go whole to the full variant (1), or
 // through the fast one, which defers every point whose tests its filters leave
 // undecided to the full variant's pass (0).
@@ -2134,6 +2136,15 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         set_error("d3g_build: at most 2^27 points per call, offsets starting at 0");
         return D3G_ERR_INVALID_ARGUMENT;
     }
+    if (opt.level_growth != 0 && (opt.level_growth < 2 || opt.level_growth > 8)) {
+        set_error("d3g_build: level_growth must be 0 or 2-8");
+        return D3G_ERR_INVALID_ARGUMENT;
+    }
+    // BRIO levels of the build's own insertion order: each level 1/ratio times
+    // the points before it, the reference's 8 or fewer (more, shorter levels).
+    // Any insertion order gives the same cells.
+    const int growth = opt.level_growth != 0 ? opt.level_growth : 8;
+    const double level_ratio = 1.0 / double(growth);
     const bool single = nsets == 1;
     const int N = int(n);
     DevBuf<uint32_t> status;
@@ -2159,7 +2170,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     // ---- insertion order and duplicate groups ----
     DevBuf<int32_t> order;
     D3G_TRY(order.alloc(size_t(N), s));
-    D3G_TRY(spatial_order_sets_device(d_xyz, h_off, d_off.p, nsets, order.p, s));
+    D3G_TRY(spatial_order_sets_device(d_xyz, h_off, d_off.p, nsets, order.p, s, level_ratio));
 
     DevBuf<double> vx;
     DevBuf<int32_t> vert_point, vset, voff;
@@ -2337,7 +2348,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     for (int st = 0; st < nsets; ++st) {
         if (hskips[size_t(st)].x < 0) continue;
         int64_t hb[64];
-        const int nb = multiscale_bounds(R.set_nv[size_t(st)], hb, 63);
+        const int nb = multiscale_bounds(R.set_nv[size_t(st)], hb, 63, level_ratio);
         std::vector<int>& L = levels[size_t(st)];
         L.push_back(0);
         for (int k = nb - 1; k >= 0; --k) L.push_back(int(hb[k]));
@@ -2379,6 +2390,17 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     // Room for the pool to grow within levels (at most one worker per 16 points).
     const bool grow = opt.chunk <= 0 && opt.split != 0;
     if (grow) maxw = std::max<int>(maxw, int(std::min<int64_t>(int64_t(nv) / 16, int64_t(1) << 18)));
+    // Asynchronous passes (see k_insert_async): a persistent grid of at most
+    // kAsyncWarps warps per level, the fast variant over the level's chunks,
+    // the full variant over what that leaves; the rounds finish the rest.
+    const bool use_async = opt.schedule != 1 && !grow;
+    constexpr int kAsyncWarps = kNumSMs * 32;   // resident at 64 registers a thread
+    // The passes over left points take all of them at once, one worker per
+    // point: the workers' own records are sized for that (wcap), the
+    // conflict-region scratch only for the warps of a pass (wslots) and the
+    // workers of a round (maxw).
+    const int wcap = use_async ? std::max<int>(maxw, int(std::min<int64_t>(nv, int64_t(1) << 20))) : maxw;
+    const int wslots = std::max(maxw, std::min(wcap, kAsyncWarps));
     Workers W;
     // Conflict-region scratch per worker (normal rounds and asynchronous
     // passes) and per big-round slot; a caller's cavity_capacity lowers both.
@@ -2392,14 +2414,14 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     DevBuf<int> wparked, wset, blist, bcount, bcav, bfac;
     DevBuf<int4> bsv, bsn;
     DevBuf<int4> wsv, wsn;
-    D3G_TRY(wcur.alloc(size_t(maxw), s));
-    D3G_TRY(wend.alloc(size_t(maxw), s));
-    D3G_TRY(wbeg.alloc(size_t(maxw), s));
-    D3G_TRY(wparked.alloc(size_t(maxw), s));
-    D3G_TRY(wset.alloc(size_t(maxw), s));
-    D3G_TRY(wpos.alloc(size_t(maxw), s));
-    D3G_TRY(wleft.alloc(size_t(maxw), s));
-    D3G_TRY(wnwon.alloc(size_t(maxw), s));
+    D3G_TRY(wcur.alloc(size_t(wcap), s));
+    D3G_TRY(wend.alloc(size_t(wcap), s));
+    D3G_TRY(wbeg.alloc(size_t(wcap), s));
+    D3G_TRY(wparked.alloc(size_t(wcap), s));
+    D3G_TRY(wset.alloc(size_t(wcap), s));
+    D3G_TRY(wpos.alloc(size_t(wcap), s));
+    D3G_TRY(wleft.alloc(size_t(wcap), s));
+    D3G_TRY(wnwon.alloc(size_t(wcap), s));
     D3G_TRY(set_p0.alloc(size_t(nsets), s));
     D3G_TRY(set_ins.alloc(size_t(nsets), s));
     D3G_TRY(set_w.alloc(size_t(nsets), s));
@@ -2407,13 +2429,13 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     D3G_TRY(nworkers.alloc(1, s));
     D3G_CUDA(cudaMemsetAsync(set_ins.p, 0, sizeof(int) * size_t(nsets), s));
     SplitState SS{set_p0.p, set_ins.p, set_w.p, set_split.p, nworkers.p, maxw};
-    D3G_TRY(wlast.alloc(size_t(maxw), s));
-    D3G_TRY(wguide.alloc(size_t(maxw), s));
-    D3G_TRY(wstate.alloc(size_t(maxw), s));
-    D3G_TRY(wncav.alloc(size_t(maxw), s));
-    D3G_TRY(wnfac.alloc(size_t(maxw), s));
-    D3G_TRY(wcav.alloc(size_t(maxw) * W.cav_cap, s));
-    D3G_TRY(wfac.alloc(size_t(maxw) * W.fac_cap, s));
+    D3G_TRY(wlast.alloc(size_t(wcap), s));
+    D3G_TRY(wguide.alloc(size_t(wcap), s));
+    D3G_TRY(wstate.alloc(size_t(wcap), s));
+    D3G_TRY(wncav.alloc(size_t(wcap), s));
+    D3G_TRY(wnfac.alloc(size_t(wcap), s));
+    D3G_TRY(wcav.alloc(size_t(wslots) * W.cav_cap, s));
+    D3G_TRY(wfac.alloc(size_t(wslots) * W.fac_cap, s));
     D3G_TRY(wsv.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(wsn.alloc(size_t(maxw) * W.fac_cap, s));
     D3G_TRY(counters.alloc(4, s));
@@ -2461,15 +2483,10 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     Rd.pstats = pstats.p;
     const int max_rounds = opt.max_rounds > 0 ? opt.max_rounds : (1 << 20);
     int round = 0;
-    // Asynchronous passes (see k_insert_async): a persistent grid of at most
-    // kAsyncWarps warps per level, the fast variant over the level's chunks,
-    // the full variant over what that leaves; the rounds finish the rest.
-    const bool use_async = opt.schedule != 1 && !grow;
-    constexpr int kAsyncWarps = kNumSMs * 32;   // resident at 64 registers a thread
     DevBuf<int> alock, anext, aleft, aleft2, anleft, apassed;
     DevBuf<unsigned long long> astats, aekey;
     if (use_async) {
-        D3G_TRY(aekey.alloc(size_t(std::min(maxw, kAsyncWarps)) * 3 * size_t(W.fac_cap), s));
+        D3G_TRY(aekey.alloc(size_t(std::min(wslots, kAsyncWarps)) * 3 * size_t(W.fac_cap), s));
         D3G_TRY(alock.alloc(size_t(T.cap), s));
         D3G_TRY(anext.alloc(1, s));
         D3G_TRY(aleft.alloc(size_t(nv), s));
@@ -2761,30 +2778,41 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 }
                 return D3G_OK;
             };
-            // The level's chunks through the fast variant, the chunks of sets
-            // whose filters are exact through the full variant; what they
-            // deferred or left (undecided tests, lock conflicts, regions too
-            // big) through the full variant, one worker per point, maxw points
-            // at a time; what that leaves through the rounds.
-            int nleft = 0, nleft2 = 0, npassed = 0;
+            // The level's chunks through the fast variant (the chunks it passes
+            // on through the full variant); what they deferred or left
+            // (undecided tests, lock conflicts, regions too big) through the
+            // full variant, one worker per point, all of them at once, again
+            // while a pass inserts at least a quarter of its points; what that
+            // leaves through the rounds, maxw points at a time.
+            int nleft = 0, npassed = 0;
             D3G_CUDA(cudaMemsetAsync(anleft.p, 0, 3 * sizeof(int), s));
             D3G_TRY(async_pass(true, nullptr, W.n, aleft.p, anleft.p, &nleft));
             D3G_CUDA(cudaMemcpyAsync(&npassed, anleft.p + 2, sizeof npassed, cudaMemcpyDeviceToHost, s));
             D3G_CUDA(cudaStreamSynchronize(s));
             if (npassed > 0) D3G_TRY(async_pass(false, apassed.p, npassed, aleft.p, anleft.p, &nleft));
             deferred = nleft;
-            for (int off = 0; off < nleft; off += maxw) {
-                W.n = std::min(maxw, nleft - off);
-                k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, aleft.p + off, W.n, vset.p, voff.p,
-                                                                        T.vert_tet);
-                D3G_TRY(async_pass(false, nullptr, W.n, aleft2.p, anleft.p + 1, &nleft2));
+            int* cur = aleft.p;
+            int* nxt = aleft2.p;
+            int ncur = nleft;
+            for (int pass = 0; ncur > 0 && pass < kLeftPasses; ++pass) {
+                int nnext = 0;
+                D3G_CUDA(cudaMemsetAsync(anleft.p + 1, 0, sizeof(int), s));
+                for (int off = 0; off < ncur; off += wcap) {
+                    W.n = std::min(wcap, ncur - off);
+                    k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, cur + off, W.n, vset.p, voff.p,
+                                                                            T.vert_tet);
+                    D3G_TRY(async_pass(false, nullptr, W.n, nxt, anleft.p + 1, &nnext));
+                }
+                const bool slow = int64_t(ncur - nnext) * 4 < int64_t(ncur);
+                std::swap(cur, nxt);
+                ncur = nnext;
+                if (slow) break;
             }
-            async_left = nleft2;
-            // What the passes left goes through the rounds, maxw points at a time.
-            for (int off = 0; off < nleft2; off += maxw) {
-                W.n = std::min(maxw, nleft2 - off);
-                k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, aleft2.p + off, W.n, vset.p,
-                                                                        voff.p, T.vert_tet);
+            async_left = ncur;
+            for (int off = 0; off < ncur; off += maxw) {
+                W.n = std::min(maxw, ncur - off);
+                k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, cur + off, W.n, vset.p, voff.p,
+                                                                        T.vert_tet);
                 D3G_TRY(run_rounds());
             }
         } else {
@@ -2973,6 +3001,7 @@ void d3g_options_default(d3g_options* o) {
     o->tet_capacity = 0;
     o->walk_limit = 0;
     o->cavity_capacity = 0;
+    o->level_growth = 0;
     // D3G_VALIDATE=1 in the environment turns the device self-check on for every
     // build that takes the defaults (as the reference's DEL3D_VALIDATE builds do).
     const char* val = getenv("D3G_VALIDATE");

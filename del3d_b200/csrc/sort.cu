@@ -770,12 +770,13 @@ int shuffle_device(int64_t n, int32_t* d_order, cudaStream_t s) {
 }
 
 /// Level boundaries of the multiscale pass: b[0] = n, b[k+1] = floor(b[k]/8)
-/// while b[k] >= 64 (spatial_sort.cpp:130-137; the ratio 0.125 is exact).
-int multiscale_bounds(int64_t n, int64_t* b, int cap) {
+/// while b[k] >= 64 (spatial_sort.cpp:130-137; the ratio 0.125 is exact).  A
+/// build may ask for another ratio (1/2 ... 1/7) for its own insertion order.
+int multiscale_bounds(int64_t n, int64_t* b, int cap, double ratio = 0.125) {
     int k = 0;
     b[k++] = n;
     while (k < cap && b[k - 1] >= 64) {
-        b[k] = int64_t(double(b[k - 1]) * 0.125);
+        b[k] = int64_t(double(b[k - 1]) * ratio);
         ++k;
     }
     return k;   // levels: [b[k+1], b[k]) for k < count-1, plus [0, b[count-1])
@@ -794,9 +795,10 @@ int upload(const std::vector<T>& v, DevBuf<T>& d, cudaStream_t s) {
 }  // namespace
 
 /// spatial_sort of every set: d_order[off[s] + p] is the local index of the
-/// point at position p of set s's insertion order.
+/// point at position p of set s's insertion order.  `level_ratio` is the
+/// multiscale ratio: the reference's 1/8, or another a build asks for.
 int spatial_order_sets_device(const double* d_xyz, const int64_t* h_off, const int64_t* d_off, int nsets,
-                              int32_t* d_order, cudaStream_t s) {
+                              int32_t* d_order, cudaStream_t s, double level_ratio = 0.125) {
     const int64_t n = h_off[nsets] - h_off[0];
     if (n <= 0) return D3G_OK;
     const bool trace = getenv("D3G_TRACE") != nullptr;
@@ -828,7 +830,7 @@ int spatial_order_sets_device(const double* d_xyz, const int64_t* h_off, const i
         const int64_t base = h_off[st], ns = h_off[st + 1] - h_off[st];
         if (ns < 2) continue;
         int64_t hb[64];
-        const int nb = multiscale_bounds(ns, hb, 63);
+        const int nb = multiscale_bounds(ns, hb, 63, level_ratio);
         for (int k = 0; k < nb; ++k) {
             const int64_t lo = k + 1 < nb ? hb[k + 1] : 0;
             classify(Seg{int(base + lo), int(base + hb[k]), 0, 0, 0, 0});

@@ -190,6 +190,11 @@ typedef struct d3g_options {
                              /* cached tet containing it; the first violation    */
                              /* ends the build with D3G_ERR_INTERNAL and its     */
                              /* description in d3g_last_error()                  */
+    int32_t level_growth;    /* points of a BRIO level over the points before it */
+    /* in the build's own insertion order: 8 (the reference's multiscale ratio  */
+    /* 1/8), or 2-7 for more, shorter levels, which a build too small to fill   */
+    /* the GPU finishes sooner; 0 = default (chosen by the build's size).  The  */
+    /* cells do not depend on it.                                               */
 } d3g_options;
 
 /* What a build did (filled by d3g_build and d3g_build_device). */

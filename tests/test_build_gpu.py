@@ -99,3 +99,30 @@ def test_schedules_and_lane_counts_agree(cuda, dist):
                    {"schedule": 0, "chunk": -12, "alpha_small": 12}):
             other, nv2 = d3.build_device(x, **kw)
             assert nv2 == nv and torch.equal(other, base), (dist, seed, kw)
+
+
+@pytest.mark.parametrize("case", ["lattice12", "sphere_q1024", "dup_grid", "uniform20k", "box5", "random500"])
+def test_level_growth_same_cells(cuda, case):
+    """The BRIO level growth of the build's insertion order (the reference's 8,
+    or 2-7 for more and shorter levels) changes the order only: the canonical
+    cells and the vertex count equal the reference's for every growth."""
+    import torch
+
+    pts = CASES[case]()
+    r, want, _ = reference(pts)
+    x = torch.from_numpy(np.ascontiguousarray(pts)).to(cuda)
+    for g in (2, 3, 4, 8):
+        cells, nv = d3.build_device(x, level_growth=g)
+        got = oracle.canonical_cells(cells.cpu().numpy())
+        assert nv == r["n_vertices"] and np.array_equal(got, want), (case, g)
+
+
+def test_level_growth_out_of_range(cuda):
+    import torch
+
+    x = torch.from_numpy(d3.gen_uniform(1000, 3)).to(cuda)
+    for g in (1, 9, -2):
+        with pytest.raises(d3.Del3dError):
+            d3.build_device(x, level_growth=g)
+    cells, _ = d3.build_device(x)
+    assert cells.shape[0] > 0
