@@ -370,13 +370,13 @@ def run_reference(args):
 # ---- ours ----------------------------------------------------------------------------
 
 
-# Measured DRAM traffic of the insertion kernel per point it inserts, from the
-# one-kernel ncu capture summarised in profiles/k_insert_async_batched256_finest.md
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch / the points that
-# launch inserted; a 256-set case of this workload, whose traffic per inserted
-# point stays the same at full size: every insertion does the same work on a
-# table much larger than L2).
-INSERT_DRAM_BYTES_PER_POINT = 16463.0
+# Measured DRAM traffic of the insertion kernel per point it inserts, from a
+# one-kernel ncu capture: dram__bytes_read.sum + dram__bytes_write.sum of the
+# fast variant's launch at the finest level of a 256-set case of this workload
+# (2.22 GB + 2.30 GB), over the 692,906 points that launch inserted.  Traffic
+# per inserted point stays the same at full size: every insertion does the same
+# kind of work on a tet table much larger than L2.
+INSERT_DRAM_BYTES_PER_POINT = 6518.0
 # Algorithmic bytes of the build per point: the coordinates read (24 B) plus the
 # finite tets written (6.75 per point x 16 B).
 BUILD_BYTES_PER_POINT = 24.0 + 6.75 * 16.0

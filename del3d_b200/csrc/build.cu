@@ -2397,8 +2397,8 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     constexpr int kAsyncWarps = kNumSMs * 32;   // resident at 64 registers a thread
     // The passes over left points take all of them at once, one worker per
     // point: the workers' own records are sized for that (wcap), the
-    // conflict-region scratch only for the warps of a pass (wslots) and the
-    // workers of a round (maxw).
+    // per-slot scratch (conflict region, boundary facets, staged tets) for the
+    // warps of a pass and the workers of a round, whichever is more (wslots).
     const int wcap = use_async ? std::max<int>(maxw, int(std::min<int64_t>(nv, int64_t(1) << 20))) : maxw;
     const int wslots = std::max(maxw, std::min(wcap, kAsyncWarps));
     Workers W;
@@ -2436,8 +2436,8 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     D3G_TRY(wnfac.alloc(size_t(wcap), s));
     D3G_TRY(wcav.alloc(size_t(wslots) * W.cav_cap, s));
     D3G_TRY(wfac.alloc(size_t(wslots) * W.fac_cap, s));
-    D3G_TRY(wsv.alloc(size_t(maxw) * W.fac_cap, s));
-    D3G_TRY(wsn.alloc(size_t(maxw) * W.fac_cap, s));
+    D3G_TRY(wsv.alloc(size_t(wslots) * W.fac_cap, s));
+    D3G_TRY(wsn.alloc(size_t(wslots) * W.fac_cap, s));
     D3G_TRY(counters.alloc(4, s));
     DevBuf<unsigned long long> sums, totals, steps;
     DevBuf<unsigned> dround;
@@ -2747,6 +2747,10 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 AsyncCtx A{alock.p, anext.p, left, nleft_d, stride, wlist, nw, apassed.p, anleft.p + 2, aekey.p,
                            astats.p};
                 const int warps = std::min(nw, kAsyncWarps);
+                if (warps > wslots) {
+                    set_error("d3g_build: asynchronous pass wider than its scratch");
+                    return D3G_ERR_INTERNAL;
+                }
                 const unsigned grid = unsigned((int64_t(warps) * 32 + 127) / 128);
                 unsigned long long won0 = 0;
                 D3G_CUDA(cudaMemcpyAsync(&won0, totals.p, sizeof won0, cudaMemcpyDeviceToHost, s));

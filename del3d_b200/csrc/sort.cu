@@ -7,8 +7,9 @@
 //      * every LCG output is computed in parallel by affine jump-ahead;
 //      * a draw can only be rejected if it lies in the top n values of the
 //        31-bit range, so only those few "candidate" draws are compacted and
-//        scanned in order by one thread, which fixes which draws are rejected
-//        (and so which draw each step consumes);
+//        scanned in order by one thread (from tiles a block stages in shared
+//        memory), which fixes which draws are rejected (and so which draw each
+//        step consumes);
 //      * the permutation follows from the j_k without replaying the swaps: the
 //        value that ends at position p is the last step m > p with j_m = p,
 //        else what step p moved there - the predecessor of p among the steps
@@ -72,25 +73,58 @@ __global__ void k_candidates(const uint32_t* __restrict__ outs, int64_t T, uint3
     }
 }
 
-/// One thread: walks the (sorted) candidate draws in order and decides which
-/// are rejected.  Draw t is consumed by step t + 1 - (rejections before t).
-__global__ void k_reject_scan(const uint32_t* __restrict__ outs, const int32_t* __restrict__ cand,
-                              const unsigned long long* ncand, int64_t n,
-                              uint8_t* __restrict__ rejected, int64_t* nrej) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int64_t s = 0;
+/// Walks the (sorted) candidate draws in order and decides which are rejected:
+/// draw t is consumed by step k = t + 1 - (rejections before t) and rejected if
+/// r / (2^31 / (k + 1)) > k (rand48.h:115-127).  The decisions chain through the
+/// rejection count, so one thread makes them; the block first stages a tile of
+/// candidates and their draws in shared memory, so that the thread's loop waits
+/// on no global load.  A draw below 2^31 - k is accepted without the division:
+/// the rejected range, 2^31 mod (k + 1) values at the top, holds at most k.
+constexpr int kRejectTile = 4096;
+__global__ void __launch_bounds__(1024) k_reject_scan(const uint32_t* __restrict__ outs,
+                                                      const int32_t* __restrict__ cand,
+                                                      const unsigned long long* ncand, int64_t n,
+                                                      uint8_t* __restrict__ rejected, int64_t* nrej) {
+    __shared__ uint32_t val[kRejectTile];
+    __shared__ int32_t pos[kRejectTile];
+    __shared__ long long s_total;
+    __shared__ int stop;
     const int64_t nc = int64_t(*ncand);
-    for (int64_t i = 0; i < nc; ++i) {
-        const int64_t t = cand[i];
-        const int64_t k = t + 1 - s;
-        if (k > n - 1) break;
-        const uint64_t bucket = (uint64_t(1) << 31) / uint64_t(k + 1);
-        if (uint64_t(outs[t]) / bucket > uint64_t(k)) {
-            rejected[t] = 1;
-            ++s;
-        }
+    if (threadIdx.x == 0) {
+        s_total = 0;
+        stop = 0;
     }
-    *nrej = s;
+    __syncthreads();
+    for (int64_t base = 0; base < nc && !stop; base += kRejectTile) {
+        const int cnt = int(nc - base < kRejectTile ? nc - base : kRejectTile);
+        for (int i = int(threadIdx.x); i < cnt; i += blockDim.x) {
+            const int32_t t = cand[base + i];
+            pos[i] = t;
+            val[i] = outs[t];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t s = s_total;
+            for (int i = 0; i < cnt; ++i) {
+                const int64_t t = pos[i];
+                const int64_t k = t + 1 - s;
+                if (k > n - 1) {
+                    stop = 1;
+                    break;
+                }
+                const uint32_t r = val[i];
+                if (r < (1u << 31) - uint32_t(k)) continue;
+                const uint64_t bucket = (uint64_t(1) << 31) / uint64_t(k + 1);
+                if (uint64_t(r) / bucket > uint64_t(k)) {
+                    rejected[t] = 1;
+                    ++s;
+                }
+            }
+            s_total = s;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *nrej = s_total;
 }
 
 __global__ void k_accept_flags(const uint8_t* __restrict__ rejected, int64_t T,
@@ -541,23 +575,25 @@ struct Seg {
     int begin, end, x, ux, uy, uz;   // recursive_sort(begin, end, x, upx, upy, upz)
 };
 
+/// A range of at most kSmall points in shared memory: coordinates and indices
+/// stay where they were loaded; the splits permute `perm`, the range's order
+/// (position -> loaded slot).
 struct Local {
-    int32_t* idx;
-    double* c[3];
+    const double* c[3];
+    uint16_t* perm;
 };
 
-__device__ void local_swap(Local& L, int i, int j) {
-    const int32_t ti = L.idx[i];
-    L.idx[i] = L.idx[j];
-    L.idx[j] = ti;
-    for (int a = 0; a < 3; ++a) {
-        const double tc = L.c[a][i];
-        L.c[a][i] = L.c[a][j];
-        L.c[a][j] = tc;
-    }
+__device__ __forceinline__ double local_coord(const Local& L, int axis, int j) {
+    return L.c[axis][L.perm[j]];
 }
 
-/// spatial_sort.cpp:40-79, verbatim in shared memory; [left, end).
+__device__ __forceinline__ void local_swap(Local& L, int i, int j) {
+    const uint16_t t = L.perm[i];
+    L.perm[i] = L.perm[j];
+    L.perm[j] = t;
+}
+
+/// spatial_sort.cpp:40-79, verbatim in shared memory by one lane; [begin, end).
 __device__ int local_split(Local& L, int begin, int end, int axis, int up) {
     if (begin >= end) return begin;
     const int middle = begin + (end - begin) / 2;
@@ -566,10 +602,10 @@ __device__ int local_split(Local& L, int begin, int end, int axis, int up) {
     for (;;) {
         const int pm = left + (right - left) / 2;
         local_swap(L, pm, right);
-        const double P = L.c[axis][right];
+        const double P = local_coord(L, axis, right);
         int result = left;
         for (int it = left; it != right; ++it) {
-            if (before_pivot(L.c[axis][it], P, up)) {
+            if (before_pivot(local_coord(L, axis, it), P, up)) {
                 local_swap(L, result, it);
                 ++result;
             }
@@ -581,6 +617,52 @@ __device__ int local_split(Local& L, int begin, int end, int axis, int up) {
     }
 }
 
+/// The same split by the whole warp: each Lomuto pass as in k_select (the
+/// elements before the pivot compacted in order by a ballot scan, the rest
+/// placed by following their chains), through `tmp` and the ranks `rk`.
+/// Every lane returns the split position.
+__device__ int warp_split(Local& L, uint16_t* tmp, int16_t* rk, int begin, int end, int axis, int up) {
+    const int lane = int(threadIdx.x & 31u);
+    const unsigned lt = (1u << lane) - 1u;
+    if (begin >= end) return begin;
+    const int middle = begin + (end - begin) / 2;
+    int left = begin, right = end - 1;
+    if (left == right) return middle;
+    for (;;) {
+        const int pm = left + (right - left) / 2;
+        if (lane == 0) local_swap(L, pm, right);
+        __syncwarp();
+        const double P = local_coord(L, axis, right);
+        int running = 0;
+        for (int base = left; base < right; base += 32) {
+            const int j = base + lane;
+            const bool less = j < right && before_pivot(local_coord(L, axis, j), P, up);
+            const unsigned m = __ballot_sync(0xffffffffu, less);
+            if (j < right) {
+                const int r = running + __popc(m & lt);
+                rk[j] = less ? int16_t(r) : int16_t(-1);
+                if (less) tmp[left + r] = L.perm[j];
+            }
+            running += __popc(m);
+        }
+        const int nl = running;
+        __syncwarp();
+        for (int q = left + nl + lane; q < right; q += 32) {
+            int x = q;
+            while (rk[x] >= 0) x = left + rk[x];
+            tmp[q == left + nl ? right : q] = L.perm[x];
+        }
+        if (lane == 0) tmp[left + nl] = L.perm[right];
+        __syncwarp();
+        for (int q = left + lane; q <= right; q += 32) L.perm[q] = tmp[q];
+        __syncwarp();
+        const int np = left + nl;
+        if (np == middle) return middle;
+        if (middle < np) right = np - 1;
+        else left = np + 1;
+    }
+}
+
 /// A node of the recursion inside a range of at most kSmall points, packed in
 /// 32 bits: begin and end (11 bits each), the axis (2 bits), the three
 /// directions (1 bit each).
@@ -589,17 +671,24 @@ __device__ __forceinline__ uint32_t pack_node(int b, int e, int x, int ux, int u
            uint32_t(uz) << 26;
 }
 
+/// A level holding at most this many nodes is split node by node by the whole
+/// warp; a fuller level, one node per lane.
+constexpr int kWarpSplitNodes = 8;
+
 /// One warp per range of at most kSmall points: the whole remaining recursion
 /// (spatial_sort.cpp:95-117) in shared memory.  The recursion's nodes cover
 /// disjoint index ranges and each one's splits read and permute only its own
 /// range, so once a node is split its eight children are independent of each
-/// other: the tree is processed level by level, the lanes taking the nodes of a
-/// level in turn, each node's seven splits done by one lane exactly as the
-/// reference does them.  The result is the reference's depth-first order, bit
-/// for bit.
+/// other: the tree is processed level by level.  The first levels (a few large
+/// nodes) are split by the whole warp, node after node; the later ones by the
+/// lanes taking the nodes of the level in turn, each node's seven splits done
+/// by one lane exactly as the reference does them.  The result is the
+/// reference's depth-first order, bit for bit.
 __global__ void __launch_bounds__(32) k_small_sort(const Seg* __restrict__ segs, Elems E) {
     __shared__ int32_t sidx[kSmall];
     __shared__ double sc[3][kSmall];
+    __shared__ uint16_t perm[kSmall], tmp[kSmall];
+    __shared__ int16_t rk[kSmall];
     // Nodes of more than 8 points at one level: fewer than kSmall / 9 + 1.
     constexpr int kNodes = kSmall / 9 + 1;
     __shared__ uint32_t nodes[2][kNodes];
@@ -611,6 +700,7 @@ __global__ void __launch_bounds__(32) k_small_sort(const Seg* __restrict__ segs,
         sc[0][j] = E.x[g.begin + j];
         sc[1][j] = E.y[g.begin + j];
         sc[2][j] = E.z[g.begin + j];
+        perm[j] = uint16_t(j);
     }
     if (threadIdx.x == 0) {
         nodes[0][0] = pack_node(0, m, g.x, g.ux, g.uy, g.uz);
@@ -618,35 +708,50 @@ __global__ void __launch_bounds__(32) k_small_sort(const Seg* __restrict__ segs,
         nnodes[1] = 0;
     }
     __syncwarp();
-    Local L{sidx, {sc[0], sc[1], sc[2]}};
+    Local L{{sc[0], sc[1], sc[2]}, perm};
     for (int cur = 0; nnodes[cur] > 0; cur ^= 1) {
         const int nxt = cur ^ 1;
         const int count = nnodes[cur];
-        for (int k = threadIdx.x; k < count; k += 32) {
+        const bool whole_warp = count <= kWarpSplitNodes;
+        for (int k = whole_warp ? 0 : int(threadIdx.x); k < count; k += whole_warp ? 1 : 32) {
             const uint32_t f = nodes[cur][k];
             const int m0 = int(f & 0x7FFu), m8 = int((f >> 11) & 0x7FFu), x = int((f >> 22) & 3u);
             const int ux = int((f >> 24) & 1u), uy = int((f >> 25) & 1u), uz = int((f >> 26) & 1u);
             const int y = (x + 1) % 3, z = (x + 2) % 3;
-            const int m4 = local_split(L, m0, m8, x, ux);
-            const int m2 = local_split(L, m0, m4, y, uy);
-            const int m1 = local_split(L, m0, m2, z, uz);
-            const int m3 = local_split(L, m2, m4, z, !uz);
-            const int m6 = local_split(L, m4, m8, y, !uy);
-            const int m5 = local_split(L, m4, m6, z, uz);
-            const int m7 = local_split(L, m6, m8, z, !uz);
-            const uint32_t ch[8] = {pack_node(m0, m1, z, uz, ux, uy),   pack_node(m1, m2, y, uy, uz, ux),
-                                    pack_node(m2, m3, y, uy, uz, ux),   pack_node(m3, m4, x, ux, !uy, !uz),
-                                    pack_node(m4, m5, x, ux, !uy, !uz), pack_node(m5, m6, y, !uy, uz, !ux),
-                                    pack_node(m6, m7, y, !uy, uz, !ux), pack_node(m7, m8, z, !uz, !ux, uy)};
-            const int lo[8] = {m0, m1, m2, m3, m4, m5, m6, m7}, hi[8] = {m1, m2, m3, m4, m5, m6, m7, m8};
-            for (int c = 0; c < 8; ++c)
-                if (hi[c] - lo[c] > 8) nodes[nxt][atomicAdd(&nnodes[nxt], 1)] = ch[c];
+            int m1, m2, m3, m4, m5, m6, m7;
+            if (whole_warp) {
+                m4 = warp_split(L, tmp, rk, m0, m8, x, ux);
+                m2 = warp_split(L, tmp, rk, m0, m4, y, uy);
+                m1 = warp_split(L, tmp, rk, m0, m2, z, uz);
+                m3 = warp_split(L, tmp, rk, m2, m4, z, !uz);
+                m6 = warp_split(L, tmp, rk, m4, m8, y, !uy);
+                m5 = warp_split(L, tmp, rk, m4, m6, z, uz);
+                m7 = warp_split(L, tmp, rk, m6, m8, z, !uz);
+            } else {
+                m4 = local_split(L, m0, m8, x, ux);
+                m2 = local_split(L, m0, m4, y, uy);
+                m1 = local_split(L, m0, m2, z, uz);
+                m3 = local_split(L, m2, m4, z, !uz);
+                m6 = local_split(L, m4, m8, y, !uy);
+                m5 = local_split(L, m4, m6, z, uz);
+                m7 = local_split(L, m6, m8, z, !uz);
+            }
+            if (!whole_warp || threadIdx.x == 0) {
+                const uint32_t ch[8] = {pack_node(m0, m1, z, uz, ux, uy),   pack_node(m1, m2, y, uy, uz, ux),
+                                        pack_node(m2, m3, y, uy, uz, ux),   pack_node(m3, m4, x, ux, !uy, !uz),
+                                        pack_node(m4, m5, x, ux, !uy, !uz), pack_node(m5, m6, y, !uy, uz, !ux),
+                                        pack_node(m6, m7, y, !uy, uz, !ux), pack_node(m7, m8, z, !uz, !ux, uy)};
+                const int lo[8] = {m0, m1, m2, m3, m4, m5, m6, m7}, hi[8] = {m1, m2, m3, m4, m5, m6, m7, m8};
+                for (int c = 0; c < 8; ++c)
+                    if (hi[c] - lo[c] > 8) nodes[nxt][atomicAdd(&nnodes[nxt], 1)] = ch[c];
+            }
+            if (whole_warp) __syncwarp();
         }
         __syncwarp();
         if (threadIdx.x == 0) nnodes[cur] = 0;
         __syncwarp();
     }
-    for (int j = threadIdx.x; j < m; j += 32) E.idx[g.begin + j] = sidx[j];
+    for (int j = threadIdx.x; j < m; j += 32) E.idx[g.begin + j] = sidx[perm[j]];
 }
 
 __global__ void k_gather_xyz(const double* __restrict__ xyz, const int32_t* __restrict__ order, int64_t n,
@@ -717,7 +822,7 @@ int shuffle_sets_device(const int64_t* h_off, const int64_t* d_off, int nsets, i
                                                     bits_for(uint64_t(T)), s));
             D3G_CUDA(cudaMemcpyAsync(cand.p, sorted.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToDevice, s));
         }
-        k_reject_scan<<<1, 32, 0, s>>>(outs.p, cand.p, ncand.p, n, rej.p, nrej.p);
+        k_reject_scan<<<1, 1024, 0, s>>>(outs.p, cand.p, ncand.p, n, rej.p, nrej.p);
         int64_t R = 0;
         D3G_CUDA(cudaMemcpyAsync(&R, nrej.p, sizeof R, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaStreamSynchronize(s));
