@@ -731,6 +731,8 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
 constexpr int kAsyncRetries = 6;
 // Passes of the full variant over a level's left points before the rounds.
 constexpr int kLeftPasses = 8;
+// BRIO level growth of the build's own order when a set's filters are exact.
+constexpr int kExactSetGrowth = 4;
 // Chunks of sets whose filters are exact go whole to the full variant (1), or
 // through the fast one, which defers every point whose tests its filters leave
 // undecided to the full variant's pass (0).
@@ -1745,6 +1747,32 @@ __device__ __forceinline__ int set_of(const int64_t* __restrict__ off, int nsets
     return lo;
 }
 
+/// Per set, the exponent span of its input coordinates, before any ordering
+/// (as k_set_span; duplicates do not change it).
+__global__ void k_raw_span(const double* __restrict__ xyz, const int64_t* __restrict__ off, int nsets, int64_t n,
+                           int* __restrict__ smin, int* __restrict__ stop) {
+    constexpr int kRun = 64;
+    const int64_t first = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * kRun;
+    if (first >= n) return;
+    const int64_t last = min(n, first + kRun);
+    int set = set_of(off, nsets, first);
+    Span sp;
+    for (int64_t p = first; p <= last; ++p) {
+        if (p == last || p >= off[set + 1]) {
+            if (!sp.empty()) {
+                atomicMin(smin + set, sp.emin);
+                atomicMax(stop + set, sp.top);
+            }
+            if (p == last) break;
+            while (p >= off[set + 1]) ++set;
+            sp = Span();
+        }
+        sp.add(xyz[3 * p]);
+        sp.add(xyz[3 * p + 1]);
+        sp.add(xyz[3 * p + 2]);
+    }
+}
+
 /// Global index of the input point at rank r (position r of its set's order).
 __device__ __forceinline__ int64_t point_at(const int32_t* __restrict__ order, const int64_t* __restrict__ off,
                                             int nsets, int64_t r) {
@@ -2140,11 +2168,6 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         set_error("d3g_build: level_growth must be 0 or 2-8");
         return D3G_ERR_INVALID_ARGUMENT;
     }
-    // BRIO levels of the build's own insertion order: each level 1/ratio times
-    // the points before it, the reference's 8 or fewer (more, shorter levels).
-    // Any insertion order gives the same cells.
-    const int growth = opt.level_growth != 0 ? opt.level_growth : 8;
-    const double level_ratio = 1.0 / double(growth);
     const bool single = nsets == 1;
     const int N = int(n);
     DevBuf<uint32_t> status;
@@ -2168,15 +2191,43 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     std::optional<NvtxRange> nvtx_phase;
     nvtx_phase.emplace("d3g.order");
     // ---- insertion order and duplicate groups ----
+    // BRIO levels of the build's own insertion order: each level `growth` times
+    // the points before it.  Any order gives the same cells, so the build may
+    // take more and shorter levels than the reference's 8, as it does by default
+    // when a set's coordinates make the filters exact (lattices and coarse grids,
+    // whose long levels collide most).  The one thing the reference's order
+    // decides is which copy of a repeated point keeps its index (the last one in
+    // that order), so input with repeated points is ordered again by it.
+    int growth = opt.level_growth;
+    if (growth == 0) {
+        DevBuf<int> span;
+        DevBuf<uint8_t> ex;
+        D3G_TRY(span.alloc(size_t(2) * size_t(nsets), s));
+        D3G_TRY(ex.alloc(size_t(nsets), s));
+        std::vector<int> init(size_t(2) * size_t(nsets));
+        for (int i = 0; i < nsets; ++i) {
+            init[size_t(i)] = 1 << 20;
+            init[size_t(nsets) + size_t(i)] = -(1 << 20);
+        }
+        D3G_CUDA(cudaMemcpyAsync(span.p, init.data(), sizeof(int) * init.size(), cudaMemcpyHostToDevice, s));
+        k_raw_span<<<grid_for((n + 63) / 64, 128, 1 << 30), 128, 0, s>>>(d_xyz, d_off.p, nsets, n, span.p,
+                                                                         span.p + nsets);
+        k_set_exact<<<grid_for(nsets, 128), 128, 0, s>>>(span.p, span.p + nsets, nsets, ex.p);
+        std::vector<uint8_t> hex(static_cast<size_t>(nsets));
+        D3G_CUDA(cudaMemcpyAsync(hex.data(), ex.p, size_t(nsets), cudaMemcpyDeviceToHost, s));
+        D3G_CUDA(cudaStreamSynchronize(s));   // `init` must outlive the copy
+        growth = 8;
+        for (const uint8_t e : hex) growth = e ? kExactSetGrowth : growth;
+    }
     DevBuf<int32_t> order;
     D3G_TRY(order.alloc(size_t(N), s));
-    D3G_TRY(spatial_order_sets_device(d_xyz, h_off, d_off.p, nsets, order.p, s, level_ratio));
 
     DevBuf<double> vx;
     DevBuf<int32_t> vert_point, vset, voff;
     int nv = N;
     D3G_TRY(voff.alloc(size_t(nsets) + 1, s));
-    {
+    for (;;) {
+        D3G_TRY(spatial_order_sets_device(d_xyz, h_off, d_off.p, nsets, order.p, s, 1.0 / double(growth)));
         DevBuf<int32_t> ranks, sranks, first, rep, vid;
         DevBuf<unsigned long long> keys, keys2;
         DevBuf<int> ndup;
@@ -2204,6 +2255,10 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         int hdup = 0;
         D3G_CUDA(cudaMemcpyAsync(&hdup, ndup.p, sizeof hdup, cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaStreamSynchronize(s));
+        if (hdup > 0 && growth != 8) {
+            growth = 8;
+            continue;
+        }
         nv = N - hdup;
         D3G_TRY(vx.alloc(size_t(3) * nv, s));
         D3G_TRY(vert_point.alloc(size_t(nv), s));
@@ -2216,7 +2271,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                                                     hdup > 0, vx.p, vert_point.p, vset.p);
         k_voff<<<grid_for(nsets + 1, 128), 128, 0, s>>>(d_off.p, nsets, vid.p, hdup > 0, n, nv, voff.p);
         D3G_CUDA(cudaGetLastError());
+        break;
     }
+    const double level_ratio = 1.0 / double(growth);
     order.release();
     R.n_vertices = nv;
     std::vector<int32_t> hvoff(size_t(nsets) + 1);

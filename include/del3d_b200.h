@@ -192,9 +192,11 @@ typedef struct d3g_options {
                              /* description in d3g_last_error()                  */
     int32_t level_growth;    /* points of a BRIO level over the points before it */
     /* in the build's own insertion order: 8 (the reference's multiscale ratio  */
-    /* 1/8), or 2-7 for more, shorter levels, which a build too small to fill   */
-    /* the GPU finishes sooner; 0 = default (chosen by the build's size).  The  */
-    /* cells do not depend on it.                                               */
+    /* 1/8) or 2-7 (more, shorter levels); 0 = default: 4 when a set's          */
+    /* coordinates make the filters exact (lattices, coarse grids), else 8.     */
+    /* Input with repeated points is always ordered with 8, since the           */
+    /* reference's order decides which copy keeps its index.  The cells do not */
+    /* depend on it.                                                            */
 } d3g_options;
 
 /* What a build did (filled by d3g_build and d3g_build_device). */
