@@ -1974,7 +1974,8 @@ __global__ void k_cell_flags(const int4* __restrict__ tv, const uint8_t* __restr
 }
 
 /// Writes the flagged tets, mapped to input point indices and canonicalised,
-/// plus their sort keys (shifted by one so the infinite vertex, -1, is 0).
+/// plus (khi given) their sort keys (shifted by one so the infinite vertex, -1,
+/// is 0).
 __global__ void k_cells_out(const int4* __restrict__ tv, const int32_t* __restrict__ flag,
                             const int32_t* __restrict__ pos, int ntet,
                             const int32_t* __restrict__ vert_point, const int32_t* __restrict__ vset,
@@ -1993,10 +1994,82 @@ __global__ void k_cells_out(const int4* __restrict__ tv, const int32_t* __restri
         q = canonical(q);
         const int o = pos[t];
         cells[o] = q;
-        khi[o] = ((unsigned long long)(uint32_t(q.x + 1)) << kbits) | uint32_t(q.y + 1);
-        klo[o] = ((unsigned long long)(uint32_t(q.z + 1)) << kbits) | uint32_t(q.w + 1);
-        idx[o] = o;
+        if (khi) {
+            khi[o] = ((unsigned long long)(uint32_t(q.x + 1)) << kbits) | uint32_t(q.y + 1);
+            klo[o] = ((unsigned long long)(uint32_t(q.z + 1)) << kbits) | uint32_t(q.w + 1);
+            idx[o] = o;
+        }
     }
+}
+
+// ---- canonical order of the finite cells by buckets ---------------------------------
+//
+// A canonical cell leads with its smallest vertex, so the lexicographic order
+// is: by that vertex, then by the other three.  The cells are bucketed by the
+// global index of their first vertex (set offset + local index; the sets are
+// contiguous, so this also orders them by set) with a counting sort, then each
+// bucket - the few cells whose smallest vertex is that point - is sorted by its
+// other three vertices.
+
+/// Buckets larger than this are left to the radix sort of every cell.
+constexpr int kBucketMax = 256;
+
+__device__ __forceinline__ int cell_bucket(const int4& q, const int32_t* __restrict__ cset,
+                                           const int64_t* __restrict__ off, int64_t o) {
+    return int(cset ? off[cset[o]] : 0) + q.x;
+}
+
+__global__ void k_bucket_count(const int4* __restrict__ cells, const int32_t* __restrict__ cset,
+                               const int64_t* __restrict__ off, int64_t n, int* __restrict__ count) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x)
+        atomicAdd(count + cell_bucket(cells[i], cset, off, i), 1);
+}
+
+__global__ void k_bucket_place(const int4* __restrict__ cells, const int32_t* __restrict__ cset,
+                               const int64_t* __restrict__ off, int64_t n, const int* __restrict__ start,
+                               int* __restrict__ fill, int4* __restrict__ out) {
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const int4 q = cells[i];
+        const int b = cell_bucket(q, cset, off, i);
+        out[start[b] + atomicAdd(fill + b, 1)] = q;
+    }
+}
+
+__device__ __forceinline__ bool cell_tail_less(const int4& a, const int4& b) {
+    if (a.y != b.y) return a.y < b.y;
+    if (a.z != b.z) return a.z < b.z;
+    return a.w < b.w;
+}
+
+/// One thread per bucket: insertion sort by the last three vertices; a bucket
+/// of more than kBucketMax cells only raises `big`.
+__global__ void k_bucket_sort(int4* __restrict__ cells, const int* __restrict__ start, int nb,
+                              int* __restrict__ big) {
+    for (int b = int(blockIdx.x) * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int lo = start[b], hi = start[b + 1];
+        if (hi - lo > kBucketMax) {
+            *big = 1;
+            continue;
+        }
+        for (int i = lo + 1; i < hi; ++i) {
+            const int4 x = cells[i];
+            int j = i - 1;
+            while (j >= lo && cell_tail_less(x, cells[j])) {
+                cells[j + 1] = cells[j];
+                --j;
+            }
+            cells[j + 1] = x;
+        }
+    }
+}
+
+/// cell_off[s] = the first bucket of set s.
+__global__ void k_cell_off(const int* __restrict__ start, const int64_t* __restrict__ off, int nsets,
+                           int64_t* __restrict__ cell_off) {
+    for (int s = int(blockIdx.x) * blockDim.x + threadIdx.x; s <= nsets; s += gridDim.x * blockDim.x)
+        cell_off[s] = start[off[s]];
 }
 
 __global__ void k_gather_cells(const int4* __restrict__ in, const int32_t* __restrict__ idx, int64_t n,
@@ -2057,20 +2130,6 @@ __global__ void k_voff(const int64_t* __restrict__ off, int nsets, const int32_t
     for (int s = int(blockIdx.x) * blockDim.x + threadIdx.x; s <= nsets; s += gridDim.x * blockDim.x) {
         const int64_t o = off[s];
         voff[s] = o >= n ? nv : (dups ? vid[o] : int32_t(o));
-    }
-}
-
-/// off[s] = first position of set s in the sorted set ids (lower bound).
-__global__ void k_set_bounds(const int32_t* __restrict__ sorted_set, int64_t n, int nsets,
-                             int64_t* __restrict__ off) {
-    for (int s = int(blockIdx.x) * blockDim.x + threadIdx.x; s <= nsets; s += gridDim.x * blockDim.x) {
-        int64_t lo = 0, hi = n;
-        while (lo < hi) {
-            const int64_t mid = (lo + hi) >> 1;
-            if (sorted_set[mid] < s) lo = mid + 1;
-            else hi = mid;
-        }
-        off[s] = lo;
     }
 }
 
@@ -2957,25 +3016,51 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         D3G_TRY(klo.alloc(size_t(nc), s));
         D3G_TRY(idx.alloc(size_t(nc), s));
         if (!single) D3G_TRY(cset.alloc(size_t(nc), s));
-        k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, vset.p, kbits,
-                                                        raw.p, khi.p, klo.p, idx.p, single ? nullptr : cset.p);
         if (!with_inf) {
-            D3G_TRY(sort_cells(raw, khi, klo, idx, single ? nullptr : cset.p, nsets, nc, kbits, R.cells, s));
-            R.n_cells = nc;
-            if (single) {
-                R.cell_off[1] = nc;
-            } else {
+            // Buckets by first vertex; the radix sort of every cell only if a
+            // bucket is too large for one thread.
+            k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, vset.p,
+                                                            kbits, raw.p, nullptr, nullptr, nullptr,
+                                                            single ? nullptr : cset.p);
+            DevBuf<int> bstart, bfill, big;
+            D3G_TRY(bstart.alloc(size_t(N) + 1, s));
+            D3G_TRY(bfill.alloc(size_t(N) + 1, s));
+            D3G_TRY(big.alloc(1, s));
+            D3G_TRY(R.cells.alloc(size_t(nc), s));
+            D3G_CUDA(cudaMemsetAsync(bfill.p, 0, sizeof(int) * (size_t(N) + 1), s));
+            D3G_CUDA(cudaMemsetAsync(big.p, 0, sizeof(int), s));
+            if (nc > 0) {
+                k_bucket_count<<<grid_for(nc, 256), 256, 0, s>>>(raw.p, single ? nullptr : cset.p, d_off.p, nc,
+                                                                 bfill.p);
+            }
+            D3G_TRY(exclusive_scan(bfill.p, bstart.p, int64_t(N) + 1, s));
+            D3G_CUDA(cudaMemsetAsync(bfill.p, 0, sizeof(int) * (size_t(N) + 1), s));
+            if (nc > 0) {
+                k_bucket_place<<<grid_for(nc, 256), 256, 0, s>>>(raw.p, single ? nullptr : cset.p, d_off.p, nc,
+                                                                 bstart.p, bfill.p, R.cells.p);
+                k_bucket_sort<<<grid_for(N, 128), 128, 0, s>>>(R.cells.p, bstart.p, N, big.p);
+            }
+            int hbig = 0;
+            D3G_CUDA(cudaMemcpyAsync(&hbig, big.p, sizeof hbig, cudaMemcpyDeviceToHost, s));
+            if (!single) {
                 DevBuf<int64_t> coff;
-                DevBuf<int32_t> sorted_set;
                 D3G_TRY(coff.alloc(size_t(nsets) + 1, s));
-                D3G_TRY(sorted_set.alloc(size_t(nc > 0 ? nc : 1), s));
-                if (nc > 0) k_gather_i32<<<grid_for(nc, 256), 256, 0, s>>>(cset.p, idx.p, nc, sorted_set.p);
-                k_set_bounds<<<grid_for(nsets + 1, 128), 128, 0, s>>>(sorted_set.p, nc, nsets, coff.p);
+                k_cell_off<<<grid_for(nsets + 1, 128), 128, 0, s>>>(bstart.p, d_off.p, nsets, coff.p);
                 D3G_CUDA(cudaMemcpyAsync(R.cell_off.data(), coff.p, sizeof(int64_t) * (size_t(nsets) + 1),
                                          cudaMemcpyDeviceToHost, s));
-                D3G_CUDA(cudaStreamSynchronize(s));
+            }
+            D3G_CUDA(cudaStreamSynchronize(s));
+            R.n_cells = nc;
+            if (single) R.cell_off[1] = nc;
+            if (hbig) {
+                k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, vset.p,
+                                                                kbits, raw.p, khi.p, klo.p, idx.p,
+                                                                single ? nullptr : cset.p);
+                D3G_TRY(sort_cells(raw, khi, klo, idx, single ? nullptr : cset.p, nsets, nc, kbits, R.cells, s));
             }
         } else {
+            k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, vset.p,
+                                                            kbits, raw.p, khi.p, klo.p, idx.p, nullptr);
             D3G_TRY(sort_cells(raw, khi, klo, idx, nullptr, 1, nc, kbits, R.all, s));
             R.n_all = nc;
         }

@@ -167,28 +167,6 @@ __global__ void k_lists(const int32_t* __restrict__ sj, const int32_t* __restric
     }
 }
 
-__global__ void k_final(const int32_t* __restrict__ j, const int32_t* __restrict__ pred,
-                        const int32_t* __restrict__ last, int64_t n, int32_t* __restrict__ order) {
-    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n;
-         p += int64_t(gridDim.x) * blockDim.x) {
-        const int32_t l = last[p];
-        if (l > p) {
-            order[p] = l;
-            continue;
-        }
-        int64_t x = p;
-        int32_t v = 0;
-        while (x > 0) {
-            const int32_t q = j[x];
-            if (q == x) { v = int32_t(x); break; }
-            const int32_t pm = pred[x];
-            if (pm > q) { v = pm; break; }
-            x = q;
-        }
-        order[p] = v;
-    }
-}
-
 /// Index of the set holding global position g: offsets[s] <= g < offsets[s+1].
 __device__ __forceinline__ int set_of(const int64_t* __restrict__ off, int nsets, int64_t g) {
     int lo = 0, hi = nsets - 1;
