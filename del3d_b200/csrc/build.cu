@@ -2011,8 +2011,10 @@ __global__ void k_cells_out(const int4* __restrict__ tv, const int32_t* __restri
 // bucket - the few cells whose smallest vertex is that point - is sorted by its
 // other three vertices.
 
-/// Buckets larger than this are left to the radix sort of every cell.
-constexpr int kBucketMax = 256;
+/// One thread sorts a bucket of up to kBucketThread cells, one block one of up
+/// to kBucketBlock; a larger bucket leaves the whole output to the radix sort.
+constexpr int kBucketThread = 32;
+constexpr int kBucketBlock = 2048;
 
 __device__ __forceinline__ int cell_bucket(const int4& q, const int32_t* __restrict__ cset,
                                            const int64_t* __restrict__ off, int64_t o) {
@@ -2043,14 +2045,19 @@ __device__ __forceinline__ bool cell_tail_less(const int4& a, const int4& b) {
     return a.w < b.w;
 }
 
-/// One thread per bucket: insertion sort by the last three vertices; a bucket
-/// of more than kBucketMax cells only raises `big`.
+/// One thread per bucket: insertion sort by the last three vertices.  A
+/// bucket of more than kBucketThread cells is listed in `mid` for
+/// k_bucket_sort_block, one of more than kBucketBlock only raises `big`.
 __global__ void k_bucket_sort(int4* __restrict__ cells, const int* __restrict__ start, int nb,
-                              int* __restrict__ big) {
+                              int* __restrict__ mid, int* __restrict__ nmid, int* __restrict__ big) {
     for (int b = int(blockIdx.x) * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
         const int lo = start[b], hi = start[b + 1];
-        if (hi - lo > kBucketMax) {
+        if (hi - lo > kBucketBlock) {
             *big = 1;
+            continue;
+        }
+        if (hi - lo > kBucketThread) {
+            mid[atomicAdd(nmid, 1)] = b;
             continue;
         }
         for (int i = lo + 1; i < hi; ++i) {
@@ -2063,6 +2070,37 @@ __global__ void k_bucket_sort(int4* __restrict__ cells, const int* __restrict__ 
             cells[j + 1] = x;
         }
     }
+}
+
+/// One block per listed bucket: a bitonic sort by the last three vertices in
+/// shared memory (padded to a power of two with cells that sort last).
+__global__ void __launch_bounds__(512) k_bucket_sort_block(int4* __restrict__ cells, const int* __restrict__ start,
+                                                           const int* __restrict__ mid) {
+    __shared__ int4 sh[kBucketBlock];
+    const int b = mid[blockIdx.x];
+    const int lo = start[b], n = start[b + 1] - lo;
+    int m = 1;
+    while (m < n) m <<= 1;
+    const int4 pad = make_int4(INT_MAX, INT_MAX, INT_MAX, INT_MAX);
+    for (int i = int(threadIdx.x); i < m; i += blockDim.x) sh[i] = i < n ? cells[lo + i] : pad;
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = int(threadIdx.x); i < m; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const int4 a = sh[i], c = sh[l];
+                    if (cell_tail_less(c, a) == up) {
+                        sh[i] = c;
+                        sh[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = int(threadIdx.x); i < n; i += blockDim.x) cells[lo + i] = sh[i];
 }
 
 /// cell_off[s] = the first bucket of set s.
@@ -3022,13 +3060,14 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, vset.p,
                                                             kbits, raw.p, nullptr, nullptr, nullptr,
                                                             single ? nullptr : cset.p);
-            DevBuf<int> bstart, bfill, big;
+            DevBuf<int> bstart, bfill, big, mid;
             D3G_TRY(bstart.alloc(size_t(N) + 1, s));
             D3G_TRY(bfill.alloc(size_t(N) + 1, s));
-            D3G_TRY(big.alloc(1, s));
+            D3G_TRY(big.alloc(2, s));
+            D3G_TRY(mid.alloc(size_t(nc / (kBucketThread + 1)) + 1, s));
             D3G_TRY(R.cells.alloc(size_t(nc), s));
             D3G_CUDA(cudaMemsetAsync(bfill.p, 0, sizeof(int) * (size_t(N) + 1), s));
-            D3G_CUDA(cudaMemsetAsync(big.p, 0, sizeof(int), s));
+            D3G_CUDA(cudaMemsetAsync(big.p, 0, 2 * sizeof(int), s));
             if (nc > 0) {
                 k_bucket_count<<<grid_for(nc, 256), 256, 0, s>>>(raw.p, single ? nullptr : cset.p, d_off.p, nc,
                                                                  bfill.p);
@@ -3038,10 +3077,10 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             if (nc > 0) {
                 k_bucket_place<<<grid_for(nc, 256), 256, 0, s>>>(raw.p, single ? nullptr : cset.p, d_off.p, nc,
                                                                  bstart.p, bfill.p, R.cells.p);
-                k_bucket_sort<<<grid_for(N, 128), 128, 0, s>>>(R.cells.p, bstart.p, N, big.p);
+                k_bucket_sort<<<grid_for(N, 128), 128, 0, s>>>(R.cells.p, bstart.p, N, mid.p, big.p + 1, big.p);
             }
-            int hbig = 0;
-            D3G_CUDA(cudaMemcpyAsync(&hbig, big.p, sizeof hbig, cudaMemcpyDeviceToHost, s));
+            int hbig[2] = {0, 0};
+            D3G_CUDA(cudaMemcpyAsync(hbig, big.p, sizeof hbig, cudaMemcpyDeviceToHost, s));
             if (!single) {
                 DevBuf<int64_t> coff;
                 D3G_TRY(coff.alloc(size_t(nsets) + 1, s));
@@ -3052,7 +3091,9 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             D3G_CUDA(cudaStreamSynchronize(s));
             R.n_cells = nc;
             if (single) R.cell_off[1] = nc;
-            if (hbig) {
+            if (!hbig[0] && hbig[1] > 0)
+                k_bucket_sort_block<<<unsigned(hbig[1]), 512, 0, s>>>(R.cells.p, bstart.p, mid.p);
+            if (hbig[0]) {
                 k_cells_out<<<grid_for(ntet, 256), 256, 0, s>>>(tv.p, flag.p, pos.p, ntet, vert_point.p, vset.p,
                                                                 kbits, raw.p, khi.p, klo.p, idx.p,
                                                                 single ? nullptr : cset.p);
