@@ -30,6 +30,11 @@ CASES = {
     "dup_copies": lambda: np.concatenate([d3.gen_uniform(5000, 2), d3.gen_uniform(5000, 2)[::3],
                                           -np.zeros((7, 3)), np.zeros((5, 3))]),
     "sphere_q_dups": lambda: d3.gen_sphere(30000, 5, q=64, dedupe=False),
+    # The centre of a sphere, first: every cell holds it, so its canonical bucket
+    # holds all cells (sorted by one block at 300 points, by the radix sort of
+    # every cell beyond 2048 cells).
+    "sphere_centre300": lambda: np.concatenate([np.zeros((1, 3)), oracle.ps_sphere(300)]),
+    "sphere_centre3000": lambda: np.concatenate([np.zeros((1, 3)), oracle.ps_sphere(3000)]),
 }
 
 
