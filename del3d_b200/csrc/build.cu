@@ -733,13 +733,6 @@ constexpr int kAsyncRetries = 6;
 constexpr int kLeftPasses = 8;
 // BRIO level growth of the build's own order when a set's filters are exact.
 constexpr int kExactSetGrowth = 4;
-// Chunks of sets whose filters are exact go whole to the full variant (1), or
-// through the fast one, which defers every point whose tests its filters leave
-// undecided to the full variant's pass (0).
-#ifndef D3G_PASS_EXACT_CHUNKS
-#define D3G_PASS_EXACT_CHUNKS 0
-#endif
-constexpr bool kPassExactChunks = D3G_PASS_EXACT_CHUNKS != 0;
 constexpr int kAsyncWalkLimit = 1 << 14;
 
 struct AsyncCtx {
@@ -747,11 +740,8 @@ struct AsyncCtx {
     int* next;                      // chunk queue head
     int* leftover;                  // points left for the rounds
     int* n_leftover;
-    int64_t stride;                 // entry q of the queue is worker (q * stride) % nw ...
-    const int* wlist;               // ... of this list (null: of all W.n workers)
+    int64_t stride;                 // entry q of the queue is worker (q * stride) % nw
     int nw;
-    int* passed;                    // kFast: workers passed on whole to the full variant
-    int* n_passed;
     unsigned long long* ekey;       // per warp slot: 3 edge keys per boundary facet (re-star)
     unsigned long long* stats;      // [0] lock conflicts, [1] walk restarts, [2] invalid seeds,
                                     // [3] regions too big, [4] points left, [5] first points left,
@@ -1378,17 +1368,8 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
         if (lane == 0) q = atomicAdd(A.next, 1);
         q = __shfl_sync(kFull, q, 0);
         if (q >= A.nw) break;
-        const int wq = int((int64_t(q) * A.stride) % A.nw);
-        const int w = A.wlist ? A.wlist[wq] : wq;
+        const int w = int((int64_t(q) * A.stride) % A.nw);
         const bool ex = W.set_exact[W.wset[w]] != 0;
-        if (kFast && ex && kPassExactChunks) {
-            // A set whose coordinates make the filters exact (integer lattices,
-            // coarse grids) needs the hull in-circle test wherever points lie in
-            // the planes of hull facets - much of the time: its chunks go whole
-            // to the full variant.
-            if (lane == 0) A.passed[atomicAdd(A.n_passed, 1)] = w;
-            continue;
-        }
         const int b = W.beg[w], len = W.end[w] - b;
         const int4 sk = W.skips[W.wset[w]];
         int pos = W.pos[w], left = W.left[w];
@@ -2637,7 +2618,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     Rd.pstats = pstats.p;
     const int max_rounds = opt.max_rounds > 0 ? opt.max_rounds : (1 << 20);
     int round = 0;
-    DevBuf<int> alock, anext, aleft, aleft2, anleft, apassed;
+    DevBuf<int> alock, anext, aleft, aleft2, anleft;
     DevBuf<unsigned long long> astats, aekey;
     if (use_async) {
         D3G_TRY(aekey.alloc(size_t(std::min(wslots, kAsyncWarps)) * 3 * size_t(W.fac_cap), s));
@@ -2645,8 +2626,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         D3G_TRY(anext.alloc(1, s));
         D3G_TRY(aleft.alloc(size_t(nv), s));
         D3G_TRY(aleft2.alloc(size_t(nv), s));
-        D3G_TRY(anleft.alloc(3, s));
-        D3G_TRY(apassed.alloc(size_t(maxw), s));
+        D3G_TRY(anleft.alloc(2, s));
         D3G_TRY(astats.alloc(7, s));
         D3G_CUDA(cudaMemsetAsync(alock.p, 0, sizeof(int) * size_t(T.cap), s));
         D3G_CUDA(cudaMemsetAsync(astats.p, 0, 7 * sizeof(unsigned long long), s));
@@ -2890,7 +2870,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
             // One asynchronous pass: a persistent grid over the workers W
             // (level chunks, or one leftover point each), writing the points it
             // leaves to `left` / `nleft_d`; their count goes to *nleft_out.
-            auto async_pass = [&](bool fast, const int* wlist, int nw, int* left, int* nleft_d,
+            auto async_pass = [&](bool fast, int nw, int* left, int* nleft_d,
                                   int* nleft_out) -> int {
                 // The chunks go out in a scattered order (stride coprime with the
                 // chunk count, near the golden ratio of it), so that chunks taken
@@ -2898,8 +2878,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 int64_t stride = std::max<int64_t>(1, int64_t(double(nw) * 0.6180339887));
                 while (std::gcd(stride, int64_t(nw)) != 1) ++stride;
                 D3G_CUDA(cudaMemsetAsync(anext.p, 0, sizeof(int), s));
-                AsyncCtx A{alock.p, anext.p, left, nleft_d, stride, wlist, nw, apassed.p, anleft.p + 2, aekey.p,
-                           astats.p};
+                AsyncCtx A{alock.p, anext.p, left, nleft_d, stride, nw, aekey.p, astats.p};
                 const int warps = std::min(nw, kAsyncWarps);
                 if (warps > wslots) {
                     set_error("d3g_build: asynchronous pass wider than its scratch");
@@ -2936,18 +2915,14 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                 }
                 return D3G_OK;
             };
-            // The level's chunks through the fast variant (the chunks it passes
-            // on through the full variant); what they deferred or left
-            // (undecided tests, lock conflicts, regions too big) through the
-            // full variant, one worker per point, all of them at once, again
-            // while a pass inserts at least a quarter of its points; what that
-            // leaves through the rounds, maxw points at a time.
-            int nleft = 0, npassed = 0;
-            D3G_CUDA(cudaMemsetAsync(anleft.p, 0, 3 * sizeof(int), s));
-            D3G_TRY(async_pass(true, nullptr, W.n, aleft.p, anleft.p, &nleft));
-            D3G_CUDA(cudaMemcpyAsync(&npassed, anleft.p + 2, sizeof npassed, cudaMemcpyDeviceToHost, s));
-            D3G_CUDA(cudaStreamSynchronize(s));
-            if (npassed > 0) D3G_TRY(async_pass(false, apassed.p, npassed, aleft.p, anleft.p, &nleft));
+            // The level's chunks through the fast variant; what it deferred or
+            // left (undecided tests, lock conflicts, regions too big) through
+            // the full variant, one worker per point, all of them at once,
+            // again while a pass inserts at least a quarter of its points; what
+            // that leaves through the rounds, maxw points at a time.
+            int nleft = 0;
+            D3G_CUDA(cudaMemsetAsync(anleft.p, 0, 2 * sizeof(int), s));
+            D3G_TRY(async_pass(true, W.n, aleft.p, anleft.p, &nleft));
             deferred = nleft;
             int* cur = aleft.p;
             int* nxt = aleft2.p;
@@ -2959,7 +2934,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
                     W.n = std::min(wcap, ncur - off);
                     k_setup_list<<<grid_for(W.n, 128, 1 << 30), 128, 0, s>>>(W, cur + off, W.n, vset.p, voff.p,
                                                                             T.vert_tet);
-                    D3G_TRY(async_pass(false, nullptr, W.n, nxt, anleft.p + 1, &nnext));
+                    D3G_TRY(async_pass(false, W.n, nxt, anleft.p + 1, &nnext));
                 }
                 const bool slow = int64_t(ncur - nnext) * 4 < int64_t(ncur);
                 std::swap(cur, nxt);
