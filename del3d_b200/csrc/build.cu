@@ -734,6 +734,10 @@ constexpr int kLeftPasses = 8;
 // BRIO level growth of the build's own order when a set's filters are exact.
 constexpr int kExactSetGrowth = 4;
 constexpr int kAsyncWalkLimit = 1 << 14;
+// The neighbour records of a warp's first kHandedTn region tets, read under
+// their locks together with their vertices, are kept in shared memory for the
+// growth step that expands them (instead of being read from L2 again there).
+constexpr int kHandedTn = 64;
 
 struct AsyncCtx {
     int* lock;                      // per tet lock word
@@ -1101,7 +1105,8 @@ __device__ __forceinline__ void facet_edge_keys(const int4 c, int i, unsigned lo
 template <bool kFast>
 __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, const AsyncCtx& A,
                             const double* __restrict__ vx, bool ex, uint32_t* st, int slot, int lane,
-                            unsigned long long* nC, unsigned long long* nF, const SharedCounters& ctr) {
+                            unsigned long long* nC, unsigned long long* nF, const SharedCounters& ctr,
+                            int4* htn) {
     const int owner = slot + 1;
     const int region = owner << 1, ring = region | 1;
     const Pt p = vpt(vx, v);
@@ -1118,6 +1123,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
     int* fac = W.fac + int64_t(slot) * W.fac_cap;
     // Seed: lock it, then check under the lock that it is alive and in conflict.
     int res = 0;   // 0 ok, 1 lock held by another, 2 not a valid seed, 3 undecided (kFast)
+
     if (lane == 0) {
         int seen = 0;
         if (!try_lock(A.lock, seed, region, &seen)) {
@@ -1129,6 +1135,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
             // build.  Only a live tet of v's own set can seed the region.
             int r = 0;
             const int4 stv = ld4(T.tv + seed);
+            htn[0] = ld4(T.tn + seed);
             if (__ldcg(T.alive + seed) && T.vset[stv.x != kInf ? stv.x : stv.y] == T.vset[v]) {
                 if (kFast) r = in_conflict_fast(T, seed, stv, p, v, vx, ex);
                 else r = conflict_test_seed(stv, p.x, p.y, p.z, v, vx, ex, st);
@@ -1157,15 +1164,19 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         const int i = lane & 3;
         int c = 0, nb = 0, kind = 0, got = -1;   // got: a tet this lane locked in this step
         bool abort = false, undecided = false;
+        int4 found_tn = make_int4(0, 0, 0, 0);
         if (valid) {
-            c = cav[head + (lane >> 2)];
-            nb = at(ld4(T.tn + c), i) >> 2;
+            const int pidx = head + (lane >> 2);
+            c = cav[pidx];
+            nb = at(pidx < kHandedTn ? htn[pidx] : ld4(T.tn + c), i) >> 2;
             int seen = 0;
             if (try_lock(A.lock, nb, ring, &seen)) {
                 got = nb;
                 int r;
-                if (kFast) r = in_conflict_fast(T, nb, ld4(T.tv + nb), p, v, vx, ex);
-                else r = conflict_test(ld4(T.tv + nb), p, v, vx, ex, st);
+                const int4 ntv = ld4(T.tv + nb);
+                found_tn = ld4(T.tn + nb);
+                if (kFast) r = in_conflict_fast(T, nb, ntv, p, v, vx, ex);
+                else r = conflict_test(ntv, p, v, vx, ex, st);
                 ctr.count(r);
                 if (r & CT_IN) {
                     LockRef(A.lock[nb]).store(region, cuda::memory_order_relaxed);
@@ -1205,6 +1216,7 @@ __device__ int insert_async(int v, int t0, const Tables& T, const Workers& W, co
         }
         if (kind == 2) cav[ncav + __popc(mc & lt)] = nb;
         if (kind == 1) fac[nfac + __popc(mf & lt)] = c * 4 + i;
+        if (kind == 2 && ncav + __popc(mc & lt) < kHandedTn) htn[ncav + __popc(mc & lt)] = found_tn;
         ncav += __popc(mc);
         nfac += __popc(mf);
         head += nproc;
@@ -1363,6 +1375,7 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
     if (slot >= nslots) return;   // the grid is rounded up to whole blocks; scratch has nslots slots
     unsigned long long won = 0, tries = 0, nC = 0, nF = 0;
     D3G_SHARED_COUNTERS(ctr);
+    __shared__ int4 handed_tn[4][kHandedTn];   // per warp of the block
     for (;;) {
         int q = 0;
         if (lane == 0) q = atomicAdd(A.next, 1);
@@ -1381,7 +1394,8 @@ __global__ void __launch_bounds__(128, 8) k_insert_async(Tables T, Workers W, As
             for (int attempt = 0; attempt < kAsyncRetries && outcome == AI_RETRY; ++attempt) {
                 if (attempt > 0) __nanosleep(200u << min(attempt, 6));
                 const int t0 = __ldcg(T.vert_tet + (last >= 0 ? last : guide));
-                outcome = insert_async<kFast>(v, t0, T, W, A, vx, ex, R.status, slot, lane, &nC, &nF, ctr);
+                outcome = insert_async<kFast>(v, t0, T, W, A, vx, ex, R.status, slot, lane, &nC, &nF, ctr,
+                                              handed_tn[threadIdx.x >> 5]);
                 ++tries;
                 if (__ldcg(R.status) != 0) outcome = AI_LEAVE;
             }
