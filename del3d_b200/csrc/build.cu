@@ -731,8 +731,10 @@ __global__ void __launch_bounds__(128, 8) k_restar(Tables T, Workers W, Round R,
 constexpr int kAsyncRetries = 6;
 // Passes of the full variant over a level's left points before the rounds.
 constexpr int kLeftPasses = 8;
-// BRIO level growth of the build's own order when a set's filters are exact.
+// BRIO level growth of the build's own order when a set's filters are exact,
+// or when the whole build has fewer than kSmallBuildPoints points.
 constexpr int kExactSetGrowth = 4;
+constexpr int64_t kSmallBuildPoints = 65536;
 constexpr int kAsyncWalkLimit = 1 << 14;
 // The neighbour records of a warp's first kHandedTn region tets, read under
 // their locks together with their vertices, are kept in shared memory for the
@@ -2287,7 +2289,8 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
     // the points before it.  Any order gives the same cells, so the build may
     // take more and shorter levels than the reference's 8, as it does by default
     // when a set's coordinates make the filters exact (lattices and coarse grids,
-    // whose long levels collide most).  The one thing the reference's order
+    // whose long levels collide most) and for a build too small to fill the GPU
+    // (whose levels are inserted chunk by chunk, so shorter ones finish sooner).  The one thing the reference's order
     // decides is which copy of a repeated point keeps its index (the last one in
     // that order), so input with repeated points is ordered again by it.
     int growth = opt.level_growth;
@@ -2308,7 +2311,7 @@ int build_sets_impl(const double* d_xyz, const int64_t* h_off, int nsets, const 
         std::vector<uint8_t> hex(static_cast<size_t>(nsets));
         D3G_CUDA(cudaMemcpyAsync(hex.data(), ex.p, size_t(nsets), cudaMemcpyDeviceToHost, s));
         D3G_CUDA(cudaStreamSynchronize(s));   // `init` must outlive the copy
-        growth = 8;
+        growth = n < kSmallBuildPoints ? kExactSetGrowth : 8;
         for (const uint8_t e : hex) growth = e ? kExactSetGrowth : growth;
     }
     DevBuf<int32_t> order;

@@ -193,7 +193,8 @@ typedef struct d3g_options {
     int32_t level_growth;    /* points of a BRIO level over the points before it */
     /* in the build's own insertion order: 8 (the reference's multiscale ratio  */
     /* 1/8) or 2-7 (more, shorter levels); 0 = default: 4 when a set's          */
-    /* coordinates make the filters exact (lattices, coarse grids), else 8.     */
+    /* coordinates make the filters exact (lattices, coarse grids) or the build */
+    /* has fewer than 65536 points, else 8.                                     */
     /* Input with repeated points is always ordered with 8, since the           */
     /* reference's order decides which copy keeps its index.  The cells do not */
     /* depend on it.                                                            */
