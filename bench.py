@@ -373,10 +373,10 @@ def run_reference(args):
 # Measured DRAM traffic of the insertion kernel per point it inserts, from a
 # one-kernel ncu capture: dram__bytes_read.sum + dram__bytes_write.sum of the
 # fast variant's launch at the finest level of a 256-set case of this workload
-# (2.22 GB + 2.30 GB), over the 692,906 points that launch inserted.  Traffic
+# (8.40 GB + 5.77 GB), over the 1,069,032 points that launch inserted.  Traffic
 # per inserted point stays the same at full size: every insertion does the same
 # kind of work on a tet table much larger than L2.
-INSERT_DRAM_BYTES_PER_POINT = 6518.0
+INSERT_DRAM_BYTES_PER_POINT = 13249.0
 # Algorithmic bytes of the build per point: the coordinates read (24 B) plus the
 # finite tets written (6.75 per point x 16 B).
 BUILD_BYTES_PER_POINT = 24.0 + 6.75 * 16.0
