@@ -168,7 +168,7 @@ struct DeviceBlockCache {
     std::multimap<size_t, IdleBlock> idle;   // size -> block not in use
     std::vector<cudaEvent_t> events;         // spare events of this device
     size_t idle_bytes = 0;
-    size_t limit = 0;                        // idle bytes kept: a quarter of the device memory
+    size_t limit = 0;                        // idle bytes kept: half the device memory
     uint64_t clock = 0;
 };
 
@@ -241,7 +241,7 @@ cudaError_t device_block_alloc(void** p, size_t bytes, cudaStream_t s, size_t* c
         if (c.limit == 0) {
             size_t free_b = 0, total_b = 0;
             if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) cudaGetLastError();
-            c.limit = std::max<size_t>(total_b / 4, size_t(1) << 30);
+            c.limit = std::max<size_t>(total_b / 2, size_t(1) << 30);
         }
         // The smallest idle block that fits, if it wastes at most a quarter.
         auto it = c.idle.lower_bound(bytes);

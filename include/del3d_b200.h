@@ -56,8 +56,8 @@ const char* d3g_last_error(void);
 
 /* The library keeps device memory it frees for later calls (builds allocate
  * gigabytes per call): blocks of 1 MiB and more in its own cache, which hands a
- * block to a later request of about its size on any stream (idle blocks up to a
- * quarter of the device memory), the rest in the current device's stream-ordered
+ * block to a later request of about its size on any stream (idle blocks up to
+ * half the device memory), the rest in the current device's stream-ordered
  * pool.  Host result arrays come from a cache of pinned blocks (freed results'
  * blocks serve later ones, up to 16 GiB).  This returns all of them to the
  * CUDA driver; it synchronises the device. */
