@@ -548,15 +548,19 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(gpu_id(torch, dev)) if rank == 0 else None
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # One event between consecutive steps: their differences give each step's
+    # time, the first and last the timed region's.
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    e0, e1 = evs[0], evs[-1]
     e0.record(stream)
     ncells = 0
     with torch.cuda.stream(stream):
-        for _ in range(args.steps):
+        for k in range(args.steps):
             cells, co, nv = step()
             ncells = int(cells.shape[0])
-    e1.record(stream)
+            evs[k + 1].record(stream)
     torch.cuda.synchronize()
+    step_ms = sorted(evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps))
     clk = clocks.stop() if clocks else None
     # After the timed region: the cells of a sample of sets, for the parity check.
     # Every rank checks the sets it built (their parity is combined below).
@@ -674,6 +678,8 @@ def run_ours(args):
                                                                    "by estimated cost n log2 n"}
                                                     if world > 1 and args.scaling == "strong" else {})),
             "tets_per_s": tets_rate,
+            "step_ms": {"min": step_ms[0], "median": step_ms[len(step_ms) // 2], "max": step_ms[-1],
+                        "note": "this rank's device time of each timed step"},
             "e2e": ({"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": 24 * n,
                      "d2h_bytes_per_step": 16 * int(e2e_cells) + 16 * len(sets) + 8}
                     if e2e_value else None),
