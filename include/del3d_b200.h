@@ -215,8 +215,9 @@ typedef struct d3g_build_stats {
     int64_t walk_steps;      /* with timing: point-location steps over all attempts  */
     int64_t bfs_steps;       /* with timing: conflict-region growth steps (8 tets each) */
     double ms_async;         /* with timing: device time of the asynchronous passes  */
-    int64_t launches_async;  /* asynchronous passes (two per level: the fast variant */
-                             /* and the full one over what it deferred)              */
+    int64_t launches_async;  /* asynchronous passes: per level the fast variant,    */
+                             /* then the full one over what it deferred or left,    */
+                             /* repeated while it inserts                           */
     int64_t async_inserted;  /* points the asynchronous passes inserted              */
     /* Conflict tests (in_sphere, or orient3d against a hull facet) the insertion
      * kernels evaluated, attempts that gave way included; of these, the ones the
